@@ -1,0 +1,405 @@
+"""rrgsim_b200 — Blackwell (sm_100a) galaxy-dynamics hot path of RRGalaxSim.
+
+Thin Python binding over the C ABI of librrg.so (include/rrg.h). Names follow the reference
+solver's free functions (solver/lib/rrgsim_nbody/include/nbody.cuh, rm_p2mesh.cuh,
+rm_mesh2p.cuh, wave.cuh) and its IntegrationSolver strategy (rrgsim_integration.cuh:22-42).
+There is no CPU fallback: if librrg.so is missing, or no CUDA device is present, the calls fail
+with RRGError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "librrg.so"
+BIN_PATH = PKG / "bin" / "rrgsim"
+
+PREC = {"fp32": 0, "mixed": 1, "fp64": 2}
+BC_ZERO_DIRICHLET, BC_PERIODIC, BC_MONOPOLE_DIRICHLET, BC_MONOPOLE_RADIATIVE = 0, 1, 2, 3
+
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "IO", 5: "STATE", 6: "UNSUPPORTED"}
+
+
+class RRGError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{STATUS.get(status, status)}] {message}")
+        self.status = status
+
+
+class SimParams(C.Structure):
+    _fields_ = [("time_max", C.c_double), ("dt_save", C.c_double), ("dt_dynamics", C.c_double),
+                ("saves_without_dump", C.c_uint64), ("use_wave_model", C.c_int32)]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("dx", C.c_double), ("domain_l", C.c_double),
+                ("domain_min", C.c_double), ("domain_max", C.c_double), ("bc_l", C.c_double),
+                ("sim_l", C.c_double)]
+
+    @classmethod
+    def from_values(cls, nx: int, dx: float, bc_frac: float = 0.0) -> "GridInfo":
+        """As from_json(GridInfo) derives the domain (solver/lib/rrgsim_io/src/io_json.cpp:28-40)."""
+        g = cls()
+        g.nx = int(nx)
+        g.dx = float(dx)
+        g.domain_l = g.dx * g.nx
+        g.sim_l = (1.0 - bc_frac) * g.domain_l
+        g.bc_l = 0.5 * bc_frac * g.domain_l
+        g.domain_max = 0.5 * g.domain_l
+        g.domain_min = -0.5 * g.domain_l
+        return g
+
+
+class WaveParams(C.Structure):
+    _fields_ = [("diss_base", C.c_double), ("diss_extra", C.c_double), ("wave_speed", C.c_double),
+                ("dt", C.c_double), ("setup_iterations", C.c_int32), ("iterations", C.c_int32),
+                ("tolerance", C.c_double), ("print_step", C.c_int32),
+                ("steady_check_step", C.c_int32), ("steady_hold_steps", C.c_int32)]
+
+    @classmethod
+    def make(cls, dx: float, diss_base: float, wave_speed: float, diss_extra: float = 0.0,
+             setup_iterations: int = 30000, iterations: int = 3000, tolerance: float = 1e-6,
+             print_step: int = 500, steady_check_step: int = 30,
+             steady_hold_steps: int = 3) -> "WaveParams":
+        """Defaults of io_json.cpp:53-99; dt from the CFL rule of io_json.cpp:170-179."""
+        w = cls()
+        w.diss_base, w.diss_extra, w.wave_speed = diss_base, diss_extra, wave_speed
+        w.dt = 0.5 * dx / (wave_speed * np.sqrt(3.0))
+        w.setup_iterations, w.iterations, w.tolerance = setup_iterations, iterations, tolerance
+        w.print_step, w.steady_check_step = print_step, steady_check_step
+        w.steady_hold_steps = steady_hold_steps
+        return w
+
+
+class Conservation(C.Structure):
+    _fields_ = [("time", C.c_double), ("Ek", C.c_double), ("Ep", C.c_double),
+                ("momentum", C.c_double * 3), ("angular", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        return {"time": self.time, "Ek": self.Ek, "Ep": self.Ep,
+                "momentum": np.array(self.momentum[:]), "angular": np.array(self.angular[:])}
+
+
+class IniParams(C.Structure):
+    _fields_ = [("mass_star", C.c_double), ("mass_dark", C.c_double), ("soft_star", C.c_double),
+                ("soft_dark", C.c_double), ("ini_file_star", C.c_char * 1024),
+                ("ini_file_dark", C.c_char * 1024)]
+
+
+class ParsedParams(C.Structure):
+    _fields_ = [("ini", IniParams), ("sim", SimParams), ("has_grid", C.c_int32),
+                ("grid", GridInfo), ("has_wave", C.c_int32), ("wave", WaveParams)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads librrg.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RRGError(2, f"{LIB_PATH} is missing: build it with `python -m rrgsim_b200.build`")
+    L = C.CDLL(str(LIB_PATH))
+    vp, d, i64, i32 = C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.c_int
+    st = C.c_int
+    sig = {
+        "rrg_version": (C.c_char_p, []),
+        "rrg_last_error": (C.c_char_p, [vp]),
+        "rrg_kernel_launch_count": (C.c_uint64, []),
+        "rrg_create": (st, [i32, i32, C.POINTER(vp)]),
+        "rrg_destroy": (st, [vp]),
+        "rrg_set_stream": (st, [vp, vp]),
+        "rrg_synchronize": (st, [vp]),
+        "rrg_load_particles": (st, [vp, i64, d, d, d, d]),
+        "rrg_num_particles": (i64, [vp]),
+        "rrg_get_particles": (st, [vp, d, d, d, d]),
+        "rrg_get_time": (st, [vp, d, C.POINTER(C.c_uint64)]),
+        "rrg_init_grid": (st, [vp, C.POINTER(GridInfo)]),
+        "rrg_set_wave_params": (st, [vp, C.POINTER(WaveParams)]),
+        "rrg_get_grid": (st, [vp, d, d, d]),
+        "rrg_set_grid_potential": (st, [vp, d]),
+        "rrg_get_deposit_scale": (st, [vp, C.POINTER(C.c_int32)]),
+        "rrg_predict_step": (st, [vp, C.c_double]),
+        "rrg_nbody_acceleration": (st, [vp]),
+        "rrg_nbody_grav": (st, [vp]),
+        "rrg_correct_step": (st, [vp, C.c_double]),
+        "rrg_convert_particles_to_grid": (st, [vp]),
+        "rrg_set_boundary_periodic": (st, [vp, C.c_double, i32]),
+        "rrg_set_boundary_monopole": (st, [vp, C.c_double, d, i32]),
+        "rrg_set_boundary_zero": (st, [vp]),
+        "rrg_solve_wave_equation": (st, [vp, i32, C.POINTER(C.c_int), d]),
+        "rrg_calc_acceleration_field": (st, [vp]),
+        "rrg_project_grid_acceleration_on_particles": (st, [vp]),
+        "rrg_project_grid_grav_on_particles": (st, [vp]),
+        "rrg_calc_conservation": (st, [vp, C.POINTER(Conservation)]),
+        "rrg_calc_mass_center": (st, [vp, d, d]),
+        "rrg_solver_init": (st, [vp, C.POINTER(SimParams)]),
+        "rrg_solver_precalc": (st, [vp]),
+        "rrg_solver_calc_steps": (st, [vp, i32]),
+        "rrg_solver_sync": (st, [vp]),
+        "rrg_set_sort_interval": (st, [vp, i32]),
+        "rrg_parse_params_json": (st, [C.c_char_p, C.POINTER(ParsedParams)]),
+        "rrg_read_ic_component": (st, [C.c_char_p, C.c_double, C.c_double, i64, i64, d, d, d, d,
+                                       C.POINTER(i64)]),
+        "rrg_ic_header_count": (st, [C.c_char_p, C.POINTER(i64)]),
+        "rrg_write_ic_text": (st, [C.c_char_p, i64, C.c_double, d, d]),
+        "rrg_write_dump": (st, [C.c_char_p, C.c_uint64, C.c_double, i64, d, d]),
+        "rrg_read_dump": (st, [C.c_char_p, i64, C.POINTER(i64), d, d, d]),
+        "rrg_run": (st, [C.c_char_p, i32, i32]),
+        "rrg_generate_plummer": (st, [C.c_uint64, i64, C.c_double, C.c_double, C.c_double, d, d]),
+        "rrg_generate_exp_disk": (st, [C.c_uint64, i64, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, d, d]),
+        "rrg_dev_direct_forces_f32": (st, [vp, vp, vp, C.c_float, i64, vp, i32, vp]),
+        "rrg_dev_direct_vjp_f32": (st, [vp, vp, C.c_float, i64, vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def check(status: int, ctx=None) -> None:
+    if status != 0:
+        msg = lib().rrg_last_error(ctx)
+        raise RRGError(status, msg.decode() if msg else "")
+
+
+def kernel_launch_count() -> int:
+    return int(lib().rrg_kernel_launch_count())
+
+
+class Context:
+    """A simulation context on one GPU (particles, optional grid, solver state)."""
+
+    def __init__(self, device: int = 0, precision: str = "fp32"):
+        self._h = C.c_void_p()
+        check(lib().rrg_create(int(device), PREC[precision], C.byref(self._h)))
+        self.precision = precision
+        self.n = 0
+        self.grid = None
+
+    # -- lifecycle ---------------------------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            lib().rrg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, status: int) -> None:
+        check(status, self._h)
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._c(lib().rrg_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def synchronize(self) -> None:
+        self._c(lib().rrg_synchronize(self._h))
+
+    # -- particles ---------------------------------------------------------------------------
+    def load_particles(self, pos, vel, mass, soft2) -> None:
+        pos, vel, mass, soft2 = _f64(pos), _f64(vel), _f64(mass), _f64(soft2)
+        n = mass.shape[0]
+        if pos.shape != (n, 3) or vel.shape != (n, 3) or soft2.shape != (n,):
+            raise RRGError(1, "load_particles: pos/vel must be (n, 3), mass/soft2 (n,)")
+        self._c(lib().rrg_load_particles(self._h, n, _d(pos), _d(vel), _d(mass), _d(soft2)))
+        self.n = n
+
+    def get_particles(self) -> dict:
+        n = self.n
+        pos, vel, acc = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        grav = np.empty(n)
+        self._c(lib().rrg_get_particles(self._h, _d(pos), _d(vel), _d(acc), _d(grav)))
+        return {"pos": pos, "vel": vel, "acc": acc, "grav": grav}
+
+    def time(self):
+        t = C.c_double()
+        it = C.c_uint64()
+        self._c(lib().rrg_get_time(self._h, C.byref(t), C.byref(it)))
+        return t.value, it.value
+
+    # -- grid --------------------------------------------------------------------------------
+    def init_grid(self, grid: GridInfo) -> None:
+        self._c(lib().rrg_init_grid(self._h, C.byref(grid)))
+        self.grid = grid
+
+    def set_wave_params(self, wave: WaveParams) -> None:
+        self._c(lib().rrg_set_wave_params(self._h, C.byref(wave)))
+
+    def get_grid(self) -> dict:
+        nc = self.grid.nx ** 3
+        mass, grav, acc = np.empty(nc), np.empty(nc), np.empty((nc, 3))
+        self._c(lib().rrg_get_grid(self._h, _d(mass), _d(grav), _d(acc)))
+        return {"mass": mass, "grav": grav, "acc": acc}
+
+    def set_grid_potential(self, phi) -> None:
+        phi = _f64(phi)
+        self._c(lib().rrg_set_grid_potential(self._h, _d(phi)))
+
+    def deposit_scale(self) -> int:
+        s = C.c_int32()
+        self._c(lib().rrg_get_deposit_scale(self._h, C.byref(s)))
+        return s.value
+
+    # -- operators (reference free functions) ------------------------------------------------
+    def predict_step(self, dt: float) -> None:
+        self._c(lib().rrg_predict_step(self._h, float(dt)))
+
+    def nbody_acceleration(self) -> None:
+        self._c(lib().rrg_nbody_acceleration(self._h))
+
+    def nbody_grav(self) -> None:
+        self._c(lib().rrg_nbody_grav(self._h))
+
+    def correct_step(self, dt: float) -> None:
+        self._c(lib().rrg_correct_step(self._h, float(dt)))
+
+    def convert_particles_to_grid(self) -> None:
+        self._c(lib().rrg_convert_particles_to_grid(self._h))
+
+    def set_boundary_periodic(self, total_mass: float, keep_layer: bool = False) -> None:
+        self._c(lib().rrg_set_boundary_periodic(self._h, float(total_mass), int(keep_layer)))
+
+    def set_boundary_monopole(self, total_mass: float, center_of_mass, radiative: bool) -> None:
+        com = _f64(center_of_mass)
+        self._c(lib().rrg_set_boundary_monopole(self._h, float(total_mass), _d(com),
+                                                int(radiative)))
+
+    def set_boundary_zero(self) -> None:
+        self._c(lib().rrg_set_boundary_zero(self._h))
+
+    def solve_wave_equation(self, max_iterations: int):
+        it = C.c_int()
+        rel = C.c_double()
+        self._c(lib().rrg_solve_wave_equation(self._h, int(max_iterations), C.byref(it),
+                                              C.byref(rel)))
+        return it.value, rel.value
+
+    def calc_acceleration_field(self) -> None:
+        self._c(lib().rrg_calc_acceleration_field(self._h))
+
+    def project_grid_acceleration_on_particles(self) -> None:
+        self._c(lib().rrg_project_grid_acceleration_on_particles(self._h))
+
+    def project_grid_grav_on_particles(self) -> None:
+        self._c(lib().rrg_project_grid_grav_on_particles(self._h))
+
+    def calc_conservation(self) -> dict:
+        c = Conservation()
+        self._c(lib().rrg_calc_conservation(self._h, C.byref(c)))
+        return c.as_dict()
+
+    def calc_mass_center(self):
+        com = np.empty(3)
+        m = C.c_double()
+        self._c(lib().rrg_calc_mass_center(self._h, _d(com), C.byref(m)))
+        return com, m.value
+
+    # -- integration strategy ----------------------------------------------------------------
+    def solver_init(self, sim: SimParams) -> None:
+        self._c(lib().rrg_solver_init(self._h, C.byref(sim)))
+
+    def precalc(self) -> None:
+        self._c(lib().rrg_solver_precalc(self._h))
+
+    def calc_steps(self, nsteps: int) -> None:
+        self._c(lib().rrg_solver_calc_steps(self._h, int(nsteps)))
+
+    def sync_particles_and_grid(self) -> None:
+        self._c(lib().rrg_solver_sync(self._h))
+
+    def set_sort_interval(self, interval: int) -> None:
+        self._c(lib().rrg_set_sort_interval(self._h, int(interval)))
+
+
+# -- host I/O --------------------------------------------------------------------------------
+def parse_params_json(path) -> ParsedParams:
+    p = ParsedParams()
+    check(lib().rrg_parse_params_json(str(path).encode(), C.byref(p)))
+    return p
+
+
+def read_ic(path, component_mass: float, component_soft: float, n_before: int = 0):
+    """One IC component; arrays sized for this file only (mass divides by n_before + N)."""
+    n = C.c_int64()
+    check(lib().rrg_ic_header_count(str(path).encode(), C.byref(n)))
+    total = n_before + n.value
+    pos, vel = np.zeros((total, 3)), np.zeros((total, 3))
+    mass, soft2 = np.zeros(total), np.zeros(total)
+    got = C.c_int64()
+    check(lib().rrg_read_ic_component(str(path).encode(), float(component_mass),
+                                      float(component_soft), int(n_before), total, _d(pos),
+                                      _d(vel), _d(mass), _d(soft2), C.byref(got)))
+    return pos[n_before:], vel[n_before:], mass[n_before:], soft2[n_before:]
+
+
+def write_ic_text(path, pos, vel, t: float = 0.0) -> None:
+    pos, vel = _f64(pos), _f64(vel)
+    check(lib().rrg_write_ic_text(str(path).encode(), pos.shape[0], float(t), _d(pos), _d(vel)))
+
+
+def write_dump(dump_dir, iteration: int, time: float, pos, vel) -> None:
+    pos, vel = _f64(pos), _f64(vel)
+    check(lib().rrg_write_dump(str(dump_dir).encode(), int(iteration), float(time), pos.shape[0],
+                               _d(pos), _d(vel)))
+
+
+def read_dump(path):
+    n = C.c_int64()
+    t = C.c_double()
+    check(lib().rrg_read_dump(str(path).encode(), 0, C.byref(n), C.byref(t), None, None))
+    pos, vel = np.empty((n.value, 3)), np.empty((n.value, 3))
+    check(lib().rrg_read_dump(str(path).encode(), n.value, C.byref(n), C.byref(t), _d(pos),
+                              _d(vel)))
+    return t.value, pos, vel
+
+
+def run(work_dir, device: int = 0, precision: str = "fp32") -> None:
+    check(lib().rrg_run(str(work_dir).encode(), int(device), PREC[precision]))
+
+
+def generate_plummer(seed: int, n: int, total_mass: float = 1.0, scale_radius: float = 1.0,
+                     r_max: float = 20.0):
+    pos, vel = np.empty((n, 3)), np.empty((n, 3))
+    check(lib().rrg_generate_plummer(int(seed), int(n), float(total_mass), float(scale_radius),
+                                     float(r_max), _d(pos), _d(vel)))
+    return pos, vel
+
+
+def generate_exp_disk(seed: int, n: int, disk_mass: float = 1.0, scale_length: float = 1.0,
+                      z0: float = 0.1, r_max: float = 7.5, z_max: float = 7.5,
+                      disp_frac: float = 0.1, bulge_mass: float = 0.0, bulge_a: float = 0.0):
+    pos, vel = np.empty((n, 3)), np.empty((n, 3))
+    check(lib().rrg_generate_exp_disk(int(seed), int(n), float(disk_mass), float(scale_length),
+                                      float(z0), float(r_max), float(z_max), float(disp_frac),
+                                      float(bulge_mass), float(bulge_a), _d(pos), _d(vel)))
+    return pos, vel
+
+
+def version() -> str:
+    return lib().rrg_version().decode()

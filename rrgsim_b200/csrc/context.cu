@@ -1,0 +1,1058 @@
+// C-ABI implementation: contexts, operators, integration strategies, CUDA graphs.
+//
+// Device state of a context (R = float for FP32/MIXED, double for FP64):
+//   posm[2]  V4<R>  (x, y, z, m)        two buffers: the fused direct step reads one, writes
+//                                         the other
+//   poslo[2] V4<float> low parts of x, y, z (MIXED)
+//   vel, acc V4<R>  synced velocity / acceleration (x_n, v_n, a_n)
+//   u        V4<R>  v + v* of the last predict (the reference's vel + vel_predicted_)
+//   pot      R      potential per particle
+//   hsoft    R      soft2 / 2 per particle (absent when all particles share one softening)
+// Grid (nx^3 cells, AT(x,y,z) = x + y nx + z nx^2):
+//   mg[2]    uint64 fixed-point cell mass (the last deposit is mg[mg_cur]; the other is zero
+//                   outside a calc_steps call)
+//   src      R      4 pi G (rho - rho_mean)
+//   phi[2]   R      potential at the current and the previous wave level
+//   acc4     V4<R>  (ax, ay, az, phi) after calc_acceleration_field
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "host_io.h"
+#include "kernels.cuh"
+
+namespace rrg {
+
+static std::atomic<uint64_t> g_launches{0};
+static thread_local bool t_capturing = false;
+static thread_local std::string t_error;
+
+void set_thread_error(const std::string& msg) { t_error = msg; }
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+bool capturing_now() { return t_capturing; }
+void set_capturing(bool on) { t_capturing = on; }
+
+int num_sms(int device) {
+    int v = 0;
+    RRG_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
+    return v;
+}
+
+// Minimal RAII device buffer.
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    Buf() = default;
+    Buf(const Buf&) = delete;
+    Buf& operator=(const Buf&) = delete;
+    ~Buf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t b) {
+        if (b == bytes && p) return;
+        release();
+        if (b == 0) return;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            (void)cudaGetLastError();
+            throw Error(RRG_ERR_NOMEM, "cudaMalloc(" + std::to_string(b) + " B) failed: " +
+                                           cudaGetErrorString(e));
+        }
+        bytes = b;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct GraphExec {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;
+};
+
+}  // namespace rrg
+
+using namespace rrg;
+
+struct rrg_ctx {
+    int device = 0;
+    int prec = RRG_PREC_FP32;
+    size_t rsz = 4;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sms = 148;
+
+    // particles
+    int64_t n = 0;
+    Buf posm[2], poslo[2], vel, acc, u, pot, hsoft, id;
+    int cur = 0;
+    bool soft_uniform = true;
+    double uniform_hsoft = 0.0;
+    double mass_max = 0.0;
+    bool sorted = false;
+    int splits = 1;
+    Buf scratch;
+
+    // grid
+    bool has_grid = false;
+    rrg_grid_info grid{};
+    GridDev gdev{};
+    Buf mg[2], src, phi[2], acc4;
+    int mg_cur = 0;
+    int phi_cur = 0;
+    bool src_dirty = true;
+    int shift_s = 0;
+    bool has_wave = false;
+    rrg_wave_params wave{};
+    int bc_type = RRG_BC_ZERO_DIRICHLET;
+    double bc_mass = 0.0, com[3] = {0, 0, 0}, r_min = 0.0, rho_mean = 0.0;
+    int keep_layer = 0;
+    Buf maxbits;
+
+    // reductions / transfers
+    Buf red_partial, red_out, dl;
+    double* host_red = nullptr;
+
+    // solver
+    bool solver_ready = false;
+    bool wave_mode = false;
+    rrg_sim_params sim{};
+    double time = 0.0;
+    uint64_t iter = 0;
+    int sort_interval = 0;
+    std::map<std::tuple<int, int, int, int>, GraphExec> graphs;
+
+    ~rrg_ctx() {
+        for (auto& kv : graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (host_red) cudaFreeHost(host_red);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    void* P() const { return posm[cur].p; }
+    void* L() const { return prec == RRG_PREC_MIXED ? poslo[cur].p : nullptr; }
+    const void* H() const { return soft_uniform ? nullptr : hsoft.p; }
+};
+
+namespace {
+
+#define RRG_ENTRY(ctx, body)                                                                  \
+    try {                                                                                     \
+        RRG_REQUIRE((ctx) != nullptr, RRG_ERR_INVALID, "null context");                       \
+        RRG_CUDA(cudaSetDevice((ctx)->device));                                               \
+        body;                                                                                 \
+        return RRG_OK;                                                                        \
+    } catch (const Error& e) {                                                                \
+        if (ctx) (ctx)->err = e.what();                                                       \
+        t_error = e.what();                                                                   \
+        return e.code;                                                                        \
+    } catch (const std::exception& e) {                                                       \
+        if (ctx) (ctx)->err = e.what();                                                       \
+        t_error = e.what();                                                                   \
+        return RRG_ERR_INVALID;                                                               \
+    }
+
+void require_particles(rrg_ctx* c) {
+    RRG_REQUIRE(c->n > 0, RRG_ERR_STATE, "no particles loaded");
+}
+void require_grid(rrg_ctx* c) {
+    RRG_REQUIRE(c->has_grid, RRG_ERR_STATE, "no grid: call rrg_init_grid first");
+}
+
+size_t v4b(const rrg_ctx* c) { return 4 * c->rsz; }
+
+void ensure_download(rrg_ctx* c, size_t bytes) {
+    if (c->dl.bytes < bytes) c->dl.alloc(bytes);
+}
+
+WaveCoef wave_coef(const rrg_ctx* c) {
+    WaveCoef w{};
+    const double C = c->wave.wave_speed, DT = c->wave.dt, DX = c->grid.dx;
+    const double diss = c->wave.diss_base;
+    const double Q = diss * C * DT * 0.5;
+    const double W = 1 + Q;
+    const double K = C * C * DT * DT / (DX * DX);
+    w.K_MAIN = K / W;
+    w.K_F = -C * C * DT * DT / W;
+    w.K_ACTUAL = 2 * (1 - 3 * K) / W;
+    w.K_OLD = (Q - 1) / W;
+    w.C = C;
+    w.DT = DT;
+    w.DX = DX;
+    w.diss_base = c->wave.diss_base;
+    w.diss_extra = c->wave.diss_extra;
+    w.sim_l = c->grid.sim_l;
+    w.domain_min = c->grid.domain_min;
+    w.bc_type = c->bc_type;
+    w.keep_layer = c->keep_layer;
+    w.rho_mean = c->rho_mean;
+    w.bc_mass = c->bc_mass;
+    w.com[0] = c->com[0];
+    w.com[1] = c->com[1];
+    w.com[2] = c->com[2];
+    w.r_min = c->r_min;
+    return w;
+}
+
+// ---------------------------------------------------------------------------------------------
+// building blocks shared by the operator calls and the fused solver steps
+// ---------------------------------------------------------------------------------------------
+void direct(rrg_ctx* c, bool want_pot, const DirectEpi& epi) {
+    DirectLaunch L;
+    L.prec = c->prec;
+    L.posm = c->P();
+    L.poslo = c->L();
+    L.hsoft = c->H();
+    L.uniform_hsoft = c->uniform_hsoft;
+    L.n = c->n;
+    L.want_pot = want_pot;
+    L.epi = epi;
+    L.splits = c->splits;
+    L.scratch = c->scratch.p;
+    L.scratch_bytes = c->scratch.bytes;
+    L.stream = c->stream;
+    launch_direct(L);
+}
+
+void wave_source(rrg_ctx* c, bool zero_other) {
+    // reads mg[mg_cur]; clears mg[1 - mg_cur] when asked (the next deposit target)
+    const double rho_sub = (c->bc_type == RRG_BC_PERIODIC) ? c->rho_mean : 0.0;
+    launch_wave_source(c->prec, c->grid.nx, c->mg[c->mg_cur].as<unsigned long long>(),
+                       c->shift_s, c->grid.dx, rho_sub, 1.0, c->src.p, false, c->stream);
+    if (zero_other) {
+        // cleared with a memset node: the source kernel must not touch the deposit it reads
+        RRG_CUDA(cudaMemsetAsync(c->mg[1 - c->mg_cur].p, 0, c->mg[1 - c->mg_cur].bytes,
+                                 c->stream));
+    }
+    c->src_dirty = false;
+}
+
+void wave_substep(rrg_ctx* c, const WaveCoef& w, unsigned long long* maxbits) {
+    launch_wave_step(c->prec, c->grid.nx, c->phi[c->phi_cur].p, c->phi[1 - c->phi_cur].p,
+                     c->src.p, w, maxbits, c->stream);
+    c->phi_cur = 1 - c->phi_cur;
+}
+
+void gradient(rrg_ctx* c) {
+    launch_gradient(c->prec, c->grid.nx, c->grid.dx, c->phi[c->phi_cur].p, c->acc4.p, c->stream);
+}
+
+PmParticleArgs pm_args(rrg_ctx* c, int deposit_target) {
+    PmParticleArgs a;
+    a.prec = c->prec;
+    a.n = c->n;
+    a.posm = c->P();
+    a.poslo = c->L();
+    a.vel = c->vel.p;
+    a.acc = c->acc.p;
+    a.u = c->u.p;
+    a.acc4 = c->acc4.p;
+    a.g = c->gdev;
+    a.shift_s = c->shift_s;
+    a.mgrid = deposit_target >= 0 ? c->mg[deposit_target].as<unsigned long long>() : nullptr;
+    a.dt = c->sim.dt_dynamics;
+    return a;
+}
+
+// Steady-state controlled relaxation (solve_wave_equation, wave.cu:230-297). Host-synchronous
+// only on check iterations.
+int solve_wave(rrg_ctx* c, int max_iterations, double* last_rel) {
+    require_grid(c);
+    RRG_REQUIRE(c->has_wave, RRG_ERR_STATE, "no wave parameters");
+    RRG_REQUIRE(max_iterations >= 0, RRG_ERR_INVALID, "max_iterations must be >= 0");
+    RRG_REQUIRE(c->wave.steady_check_step > 0, RRG_ERR_INVALID,
+                "steady_check_step must be positive (used as a modulus, wave.cu:275)");
+    if (c->src_dirty) wave_source(c, false);
+    const WaveCoef w = wave_coef(c);
+    int hold = 0;
+    double rel = -1.0;
+    int it = 0;
+    for (int iter = 0; iter < max_iterations; ++iter) {
+        const bool check = iter && (iter % c->wave.steady_check_step == 0);
+        if (check) RRG_CUDA(cudaMemsetAsync(c->maxbits.p, 0, 16, c->stream));
+        wave_substep(c, w, check ? c->maxbits.as<unsigned long long>() : nullptr);
+        it = iter + 1;
+        if (check) {
+            unsigned long long bits[2];
+            RRG_CUDA(cudaMemcpyAsync(bits, c->maxbits.p, 16, cudaMemcpyDeviceToHost, c->stream));
+            RRG_CUDA(cudaStreamSynchronize(c->stream));
+            double d, a;
+            std::memcpy(&d, &bits[0], 8);
+            std::memcpy(&a, &bits[1], 8);
+            rel = d / (a + 1e-30);
+            if (rel < c->wave.tolerance) ++hold;
+            else hold = 0;
+            if (hold >= c->wave.steady_hold_steps) break;
+        }
+    }
+    if (last_rel) *last_rel = rel;
+    return it;
+}
+
+void drop_graphs(rrg_ctx* c) {
+    for (auto& kv : c->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->graphs.clear();
+}
+
+void set_periodic(rrg_ctx* c, double total_mass, int keep_layer) {
+    drop_graphs(c);
+    const double L = c->grid.nx * c->grid.dx;
+    c->bc_type = RRG_BC_PERIODIC;
+    c->bc_mass = total_mass;
+    c->rho_mean = total_mass / (L * L * L);
+    c->keep_layer = keep_layer ? 1 : 0;
+    c->src_dirty = true;
+}
+
+void deposit_operator(rrg_ctx* c) {
+    RRG_CUDA(cudaMemsetAsync(c->mg[c->mg_cur].p, 0, c->mg[c->mg_cur].bytes, c->stream));
+    launch_cic_deposit(c->prec, c->n, c->P(), c->L(), c->gdev, c->shift_s,
+                       c->mg[c->mg_cur].as<unsigned long long>(), c->stream);
+    c->src_dirty = true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused solver steps
+// ---------------------------------------------------------------------------------------------
+// N-body: [predict] then nsteps direct-sum launches whose epilogue is correct (+ next predict).
+void record_nbody_steps(rrg_ctx* c, int nsteps) {
+    launch_predict(c->prec, c->n, c->P(), c->L(), c->vel.p, c->acc.p, c->u.p,
+                   c->sim.dt_dynamics, c->stream);
+    for (int s = 0; s < nsteps; ++s) {
+        DirectEpi e;
+        e.dt = c->sim.dt_dynamics;
+        e.u = c->u.p;
+        if (s + 1 < nsteps) {
+            e.mode = EPI_CORRECT_PREDICT;
+            e.pos_out = c->posm[1 - c->cur].p;
+            e.lo_out = c->prec == RRG_PREC_MIXED ? c->poslo[1 - c->cur].p : nullptr;
+            direct(c, false, e);
+            c->cur = 1 - c->cur;
+        } else {
+            e.mode = EPI_CORRECT;
+            e.vel = c->vel.p;
+            e.acc = c->acc.p;
+            direct(c, false, e);
+        }
+    }
+}
+
+// Wave: [predict + deposit] then per step: source, `iterations` substeps, gradient, fused
+// particle pass (interp + correct [+ next predict + deposit]).
+void record_wave_steps(rrg_ctx* c, int nsteps) {
+    const WaveCoef w = wave_coef(c);
+    {
+        const int t = 1 - c->mg_cur;  // known zero
+        PmParticleArgs a = pm_args(c, t);
+        launch_pm_particles(a, PM_PREDICT_DEPOSIT, c->stream);
+        c->mg_cur = t;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        wave_source(c, true);
+        for (int k = 0; k < c->wave.iterations; ++k) wave_substep(c, w, nullptr);
+        gradient(c);
+        if (s + 1 < nsteps) {
+            const int t = 1 - c->mg_cur;
+            PmParticleArgs a = pm_args(c, t);
+            launch_pm_particles(a, PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT, c->stream);
+            c->mg_cur = t;
+        } else {
+            PmParticleArgs a = pm_args(c, -1);
+            launch_pm_particles(a, PM_INTERP_CORRECT | PM_WRITE_SYNC, c->stream);
+        }
+    }
+}
+
+// Wave strategy step by step with steady checks inside each solve (used when a check falls
+// inside the per-step iterations, so control flow depends on device data).
+void wave_steps_unfused(rrg_ctx* c, int nsteps) {
+    for (int s = 0; s < nsteps; ++s) {
+        launch_predict(c->prec, c->n, c->P(), c->L(), c->vel.p, c->acc.p, c->u.p,
+                       c->sim.dt_dynamics, c->stream);
+        deposit_operator(c);
+        solve_wave(c, c->wave.iterations, nullptr);
+        gradient(c);
+        launch_interp(c->prec, c->n, c->P(), c->L(), c->gdev, c->acc4.p, c->acc.p, c->stream);
+        launch_correct(c->prec, c->n, c->vel.p, c->acc.p, c->u.p, c->sim.dt_dynamics, c->stream);
+    }
+}
+
+void run_graph(rrg_ctx* c, int nsteps) {
+    const auto key = std::make_tuple(nsteps, c->cur, c->mg_cur, c->phi_cur);
+    auto it = c->graphs.find(key);
+    const int cur0 = c->cur, mg0 = c->mg_cur, phi0 = c->phi_cur;
+    if (it == c->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        RRG_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        set_capturing(true);
+        try {
+            if (c->wave_mode) record_wave_steps(c, nsteps);
+            else record_nbody_steps(c, nsteps);
+        } catch (...) {
+            set_capturing(false);
+            cudaStreamEndCapture(c->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            c->cur = cur0;
+            c->mg_cur = mg0;
+            c->phi_cur = phi0;
+            throw;
+        }
+        set_capturing(false);
+        RRG_CUDA(cudaStreamEndCapture(c->stream, &g));
+        GraphExec ge;
+        size_t nn = 0;
+        RRG_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn) RRG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+        for (auto& nd : nodes) {
+            cudaGraphNodeType t;
+            RRG_CUDA(cudaGraphNodeGetType(nd, &t));
+            if (t == cudaGraphNodeTypeKernel) ++ge.kernels;
+        }
+        cudaError_t e = cudaGraphInstantiate(&ge.exec, g, 0);
+        cudaGraphDestroy(g);
+        RRG_CUDA(e);
+        it = c->graphs.emplace(key, ge).first;
+    } else {
+        // replaying: advance the buffer roles exactly as recording did
+        if (c->wave_mode) {
+            c->mg_cur = (nsteps % 2 == 1) ? 1 - mg0 : mg0;
+            if (c->wave.iterations % 2 == 1) c->phi_cur = (nsteps % 2 == 1) ? 1 - phi0 : phi0;
+        } else {
+            c->cur = ((nsteps - 1) % 2 == 1) ? 1 - cur0 : cur0;
+        }
+    }
+    RRG_CUDA(cudaGraphLaunch(it->second.exec, c->stream));
+    count_launches(it->second.kernels);
+}
+
+}  // namespace
+
+// ================================================================================================
+// C ABI
+// ================================================================================================
+extern "C" {
+
+RRG_API const char* rrg_version(void) { return "rrgsim-b200 0.1 (sm_100a)"; }
+
+RRG_API const char* rrg_last_error(const rrg_ctx* ctx) {
+    if (ctx) return ctx->err.c_str();
+    return t_error.c_str();
+}
+
+RRG_API uint64_t rrg_kernel_launch_count(void) { return g_launches.load(); }
+
+RRG_API rrg_status rrg_create(int device, int precision, rrg_ctx** out) {
+    try {
+        RRG_REQUIRE(out != nullptr, RRG_ERR_INVALID, "rrg_create: out is NULL");
+        RRG_REQUIRE(precision >= RRG_PREC_FP32 && precision <= RRG_PREC_FP64, RRG_ERR_INVALID,
+                    "rrg_create: unknown precision");
+        int count = 0;
+        RRG_CUDA(cudaGetDeviceCount(&count));
+        RRG_REQUIRE(device >= 0 && device < count, RRG_ERR_INVALID,
+                    "rrg_create: no CUDA device " + std::to_string(device));
+        RRG_CUDA(cudaSetDevice(device));
+        auto* c = new rrg_ctx();
+        c->device = device;
+        c->prec = precision;
+        c->rsz = precision == RRG_PREC_FP64 ? 8 : 4;
+        c->sms = num_sms(device);
+        cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete c;
+            RRG_CUDA(e);
+        }
+        c->stream = c->own_stream;
+        e = cudaMallocHost(&c->host_red, 16 * sizeof(double));
+        if (e != cudaSuccess) {
+            delete c;
+            RRG_CUDA(e);
+        }
+        *out = c;
+        return RRG_OK;
+    } catch (const Error& e) {
+        t_error = e.what();
+        return e.code;
+    }
+}
+
+RRG_API rrg_status rrg_destroy(rrg_ctx* ctx) {
+    if (!ctx) return RRG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+    return RRG_OK;
+}
+
+RRG_API rrg_status rrg_set_stream(rrg_ctx* ctx, void* stream) {
+    RRG_ENTRY(ctx, {
+        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    })
+}
+
+RRG_API rrg_status rrg_synchronize(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, { RRG_CUDA(cudaStreamSynchronize(ctx->stream)); })
+}
+
+RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos,
+                                      const double* vel, const double* mass,
+                                      const double* soft2) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(n >= 1, RRG_ERR_INVALID, "rrg_load_particles: n must be >= 1");
+        RRG_REQUIRE(n < (int64_t(1) << 31), RRG_ERR_INVALID,
+                    "rrg_load_particles: n must be < 2^31");
+        RRG_REQUIRE(pos && vel && mass && soft2, RRG_ERR_INVALID,
+                    "rrg_load_particles: NULL array");
+        double mmax = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            for (int k = 0; k < 3; ++k) {
+                RRG_REQUIRE(std::isfinite(pos[3 * i + k]) && std::isfinite(vel[3 * i + k]),
+                            RRG_ERR_INVALID,
+                            "rrg_load_particles: non-finite position/velocity at particle " +
+                                std::to_string(i));
+            }
+            RRG_REQUIRE(std::isfinite(mass[i]) && mass[i] >= 0.0, RRG_ERR_INVALID,
+                        "rrg_load_particles: bad mass at particle " + std::to_string(i));
+            RRG_REQUIRE(std::isfinite(soft2[i]) && soft2[i] >= 0.0, RRG_ERR_INVALID,
+                        "rrg_load_particles: bad soft2 at particle " + std::to_string(i));
+            mmax = std::max(mmax, mass[i]);
+        }
+        bool uniform = true;
+        for (int64_t i = 1; i < n && uniform; ++i) uniform = (soft2[i] == soft2[0]);
+
+        ctx->n = n;
+        ctx->cur = 0;
+        ctx->soft_uniform = uniform;
+        ctx->uniform_hsoft = 0.5 * soft2[0];
+        ctx->mass_max = mmax;
+        ctx->sorted = false;
+        ctx->time = 0.0;
+        ctx->iter = 0;
+        ctx->solver_ready = false;
+        for (auto& kv : ctx->graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        ctx->graphs.clear();
+        {
+            int e = 0;
+            std::frexp(mmax > 0 ? mmax : 1.0, &e);
+            ctx->shift_s = 26 - e;  // m_max 2^S <= 2^26: one contribution fits 27 bits
+        }
+        const size_t vb = v4b(ctx) * n;
+        ctx->posm[0].alloc(vb);
+        ctx->posm[1].alloc(vb);
+        if (ctx->prec == RRG_PREC_MIXED) {
+            ctx->poslo[0].alloc(sizeof(V4<float>) * n);
+            ctx->poslo[1].alloc(sizeof(V4<float>) * n);
+        } else {
+            ctx->poslo[0].release();
+            ctx->poslo[1].release();
+        }
+        ctx->vel.alloc(vb);
+        ctx->acc.alloc(vb);
+        ctx->u.alloc(vb);
+        ctx->pot.alloc(ctx->rsz * n);
+        if (!uniform) ctx->hsoft.alloc(ctx->rsz * n);
+        else ctx->hsoft.release();
+        ctx->id.release();
+        ctx->splits = direct_choose_splits(ctx->prec, n, ctx->sms);
+        const size_t sb = direct_scratch_bytes(ctx->prec, n, ctx->splits);
+        if (sb) ctx->scratch.alloc(sb);
+        const int rb = conservation_blocks(n);
+        ctx->red_partial.alloc(static_cast<size_t>(rb) * 12 * sizeof(double));
+        ctx->red_out.alloc(16 * sizeof(double));
+
+        // stage the FP64 host arrays, then pack on the device
+        const size_t stage = static_cast<size_t>(n) * 8 * sizeof(double);
+        ensure_download(ctx, stage);
+        double* d = ctx->dl.as<double>();
+        RRG_CUDA(cudaMemcpyAsync(d, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        RRG_CUDA(cudaMemcpyAsync(d + 3 * n, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        RRG_CUDA(cudaMemcpyAsync(d + 6 * n, mass, n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        RRG_CUDA(cudaMemcpyAsync(d + 7 * n, soft2, n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        launch_pack_state(ctx->prec, n, d, d + 3 * n, d + 6 * n, d + 7 * n, ctx->posm[0].p,
+                          ctx->poslo[0].p, ctx->vel.p, uniform ? nullptr : ctx->hsoft.p,
+                          ctx->stream);
+        RRG_CUDA(cudaMemsetAsync(ctx->acc.p, 0, vb, ctx->stream));
+        RRG_CUDA(cudaMemsetAsync(ctx->u.p, 0, vb, ctx->stream));
+        RRG_CUDA(cudaMemsetAsync(ctx->pot.p, 0, ctx->rsz * n, ctx->stream));
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+RRG_API int64_t rrg_num_particles(const rrg_ctx* ctx) { return ctx ? ctx->n : 0; }
+
+RRG_API rrg_status rrg_get_particles(rrg_ctx* ctx, double* pos, double* vel, double* acc,
+                                     double* grav) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        const int64_t n = ctx->n;
+        ensure_download(ctx, static_cast<size_t>(n) * 10 * sizeof(double));
+        double* d = ctx->dl.as<double>();
+        launch_unpack_state(ctx->prec, n, ctx->sorted ? ctx->id.as<int32_t>() : nullptr,
+                            ctx->P(), ctx->L(), ctx->vel.p, ctx->acc.p, ctx->pot.p,
+                            pos ? d : nullptr, vel ? d + 3 * n : nullptr,
+                            acc ? d + 6 * n : nullptr, grav ? d + 9 * n : nullptr, ctx->stream);
+        if (pos) RRG_CUDA(cudaMemcpyAsync(pos, d, 3 * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (vel)
+            RRG_CUDA(cudaMemcpyAsync(vel, d + 3 * n, 3 * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (acc)
+            RRG_CUDA(cudaMemcpyAsync(acc, d + 6 * n, 3 * n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (grav)
+            RRG_CUDA(cudaMemcpyAsync(grav, d + 9 * n, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+RRG_API rrg_status rrg_get_time(const rrg_ctx* ctx, double* time, uint64_t* iter) {
+    if (!ctx) return RRG_ERR_INVALID;
+    if (time) *time = ctx->time;
+    if (iter) *iter = ctx->iter;
+    return RRG_OK;
+}
+
+RRG_API rrg_status rrg_init_grid(rrg_ctx* ctx, const rrg_grid_info* grid) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(grid != nullptr, RRG_ERR_INVALID, "rrg_init_grid: NULL grid");
+        RRG_REQUIRE(grid->nx >= 2 && grid->nx <= 1024, RRG_ERR_INVALID,
+                    "rrg_init_grid: nx must be in [2, 1024]");
+        RRG_REQUIRE(grid->dx > 0 && std::isfinite(grid->dx), RRG_ERR_INVALID,
+                    "rrg_init_grid: dx must be positive");
+        ctx->grid = *grid;
+        ctx->gdev.nx = grid->nx;
+        ctx->gdev.dx = grid->dx;
+        ctx->gdev.domain_min = grid->domain_min;
+        ctx->gdev.inv_dx = 1.0 / grid->dx;
+        ctx->gdev.sim_l = grid->sim_l;
+        const size_t nc = static_cast<size_t>(grid->nx) * grid->nx * grid->nx;
+        ctx->mg[0].alloc(nc * 8);
+        ctx->mg[1].alloc(nc * 8);
+        ctx->src.alloc(nc * ctx->rsz);
+        ctx->phi[0].alloc(nc * ctx->rsz);
+        ctx->phi[1].alloc(nc * ctx->rsz);
+        ctx->acc4.alloc(nc * v4b(ctx));
+        ctx->maxbits.alloc(16);
+        for (Buf* b : {&ctx->mg[0], &ctx->mg[1], &ctx->src, &ctx->phi[0], &ctx->phi[1],
+                       &ctx->acc4, &ctx->maxbits})
+            RRG_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, ctx->stream));
+        ctx->mg_cur = 0;
+        ctx->phi_cur = 0;
+        ctx->src_dirty = true;
+        ctx->has_grid = true;
+        ctx->bc_type = RRG_BC_ZERO_DIRICHLET;
+        for (auto& kv : ctx->graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        ctx->graphs.clear();
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+RRG_API rrg_status rrg_set_wave_params(rrg_ctx* ctx, const rrg_wave_params* wave) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(wave != nullptr, RRG_ERR_INVALID, "rrg_set_wave_params: NULL");
+        RRG_REQUIRE(std::isfinite(wave->dt) && wave->dt > 0, RRG_ERR_INVALID,
+                    "rrg_set_wave_params: dt must be positive (0.5 dx / (c sqrt 3))");
+        RRG_REQUIRE(wave->iterations >= 0 && wave->setup_iterations >= 0, RRG_ERR_INVALID,
+                    "rrg_set_wave_params: negative iteration count");
+        ctx->wave = *wave;
+        ctx->has_wave = true;
+        for (auto& kv : ctx->graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        ctx->graphs.clear();
+    })
+}
+
+RRG_API rrg_status rrg_get_grid(rrg_ctx* ctx, double* mass, double* grav, double* acc) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        const size_t nc = static_cast<size_t>(ctx->grid.nx) * ctx->grid.nx * ctx->grid.nx;
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (mass) {
+            std::vector<unsigned long long> q(nc);
+            RRG_CUDA(cudaMemcpy(q.data(), ctx->mg[ctx->mg_cur].p, nc * 8, cudaMemcpyDeviceToHost));
+            const double inv = std::ldexp(1.0, -ctx->shift_s);
+            for (size_t i = 0; i < nc; ++i) mass[i] = static_cast<double>(q[i]) * inv;
+        }
+        if (grav) {
+            if (ctx->rsz == 8) {
+                RRG_CUDA(cudaMemcpy(grav, ctx->phi[ctx->phi_cur].p, nc * 8, cudaMemcpyDeviceToHost));
+            } else {
+                std::vector<float> f(nc);
+                RRG_CUDA(cudaMemcpy(f.data(), ctx->phi[ctx->phi_cur].p, nc * 4, cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < nc; ++i) grav[i] = f[i];
+            }
+        }
+        if (acc) {
+            if (ctx->rsz == 8) {
+                std::vector<V4<double>> f(nc);
+                RRG_CUDA(cudaMemcpy(f.data(), ctx->acc4.p, nc * 32, cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < nc; ++i) {
+                    acc[3 * i] = f[i].x;
+                    acc[3 * i + 1] = f[i].y;
+                    acc[3 * i + 2] = f[i].z;
+                }
+            } else {
+                std::vector<V4<float>> f(nc);
+                RRG_CUDA(cudaMemcpy(f.data(), ctx->acc4.p, nc * 16, cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < nc; ++i) {
+                    acc[3 * i] = f[i].x;
+                    acc[3 * i + 1] = f[i].y;
+                    acc[3 * i + 2] = f[i].z;
+                }
+            }
+        }
+    })
+}
+
+RRG_API rrg_status rrg_set_grid_potential(rrg_ctx* ctx, const double* grav) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        RRG_REQUIRE(grav != nullptr, RRG_ERR_INVALID, "rrg_set_grid_potential: NULL");
+        const size_t nc = static_cast<size_t>(ctx->grid.nx) * ctx->grid.nx * ctx->grid.nx;
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int k = 0; k < 2; ++k) {
+            if (ctx->rsz == 8) {
+                RRG_CUDA(cudaMemcpy(ctx->phi[k].p, grav, nc * 8, cudaMemcpyHostToDevice));
+            } else {
+                std::vector<float> f(grav, grav + nc);
+                RRG_CUDA(cudaMemcpy(ctx->phi[k].p, f.data(), nc * 4, cudaMemcpyHostToDevice));
+            }
+        }
+    })
+}
+
+RRG_API rrg_status rrg_get_deposit_scale(const rrg_ctx* ctx, int32_t* shift_s) {
+    if (!ctx || !shift_s) return RRG_ERR_INVALID;
+    *shift_s = ctx->shift_s;
+    return RRG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+RRG_API rrg_status rrg_predict_step(rrg_ctx* ctx, double dt) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        launch_predict(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->acc.p, ctx->u.p,
+                       dt, ctx->stream);
+    })
+}
+
+RRG_API rrg_status rrg_nbody_acceleration(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        DirectEpi e;
+        e.mode = EPI_STORE;
+        e.acc = ctx->acc.p;
+        direct(ctx, false, e);
+    })
+}
+
+RRG_API rrg_status rrg_nbody_grav(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        // potential only: accelerations go to the scratch download buffer and are dropped
+        ensure_download(ctx, v4b(ctx) * ctx->n);
+        DirectEpi e;
+        e.mode = EPI_STORE;
+        e.acc = ctx->dl.p;
+        e.pot = ctx->pot.p;
+        direct(ctx, true, e);
+    })
+}
+
+RRG_API rrg_status rrg_correct_step(rrg_ctx* ctx, double dt) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        launch_correct(ctx->prec, ctx->n, ctx->vel.p, ctx->acc.p, ctx->u.p, dt, ctx->stream);
+    })
+}
+
+RRG_API rrg_status rrg_convert_particles_to_grid(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        require_grid(ctx);
+        deposit_operator(ctx);
+    })
+}
+
+RRG_API rrg_status rrg_set_boundary_periodic(rrg_ctx* ctx, double total_mass, int keep_layer) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        set_periodic(ctx, total_mass, keep_layer);
+    })
+}
+
+RRG_API rrg_status rrg_set_boundary_monopole(rrg_ctx* ctx, double total_mass,
+                                             const double center_of_mass[3], int radiative) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        RRG_REQUIRE(center_of_mass != nullptr, RRG_ERR_INVALID, "NULL centre of mass");
+        drop_graphs(ctx);
+        ctx->bc_type = radiative ? RRG_BC_MONOPOLE_RADIATIVE : RRG_BC_MONOPOLE_DIRICHLET;
+        ctx->bc_mass = total_mass;
+        for (int k = 0; k < 3; ++k) ctx->com[k] = center_of_mass[k];
+        ctx->r_min = 0.5 * ctx->grid.dx;
+        ctx->rho_mean = 0.0;
+        ctx->keep_layer = 0;
+        ctx->src_dirty = true;
+    })
+}
+
+RRG_API rrg_status rrg_set_boundary_zero(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        drop_graphs(ctx);
+        ctx->bc_type = RRG_BC_ZERO_DIRICHLET;
+        ctx->rho_mean = 0.0;
+        ctx->src_dirty = true;
+    })
+}
+
+RRG_API rrg_status rrg_solve_wave_equation(rrg_ctx* ctx, int max_iterations,
+                                           int* iterations_run, double* last_rel_diff) {
+    RRG_ENTRY(ctx, {
+        const int it = solve_wave(ctx, max_iterations, last_rel_diff);
+        if (iterations_run) *iterations_run = it;
+    })
+}
+
+RRG_API rrg_status rrg_calc_acceleration_field(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        gradient(ctx);
+    })
+}
+
+RRG_API rrg_status rrg_project_grid_acceleration_on_particles(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        require_grid(ctx);
+        launch_interp(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->gdev, ctx->acc4.p, ctx->acc.p,
+                      ctx->stream);
+    })
+}
+
+RRG_API rrg_status rrg_project_grid_grav_on_particles(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        require_grid(ctx);
+        launch_ngp_phi(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->gdev,
+                       ctx->phi[ctx->phi_cur].p, ctx->pot.p, ctx->stream);
+    })
+}
+
+static void reduce_state(rrg_ctx* ctx) {
+    const int rb = conservation_blocks(ctx->n);
+    launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
+                        ctx->red_partial.as<double>(), rb, ctx->red_out.as<double>(),
+                        ctx->stream);
+    RRG_CUDA(cudaMemcpyAsync(ctx->host_red, ctx->red_out.p, 12 * sizeof(double),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+RRG_API rrg_status rrg_calc_conservation(rrg_ctx* ctx, rrg_conservation* out) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        RRG_REQUIRE(out != nullptr, RRG_ERR_INVALID, "NULL output");
+        reduce_state(ctx);
+        const double* r = ctx->host_red;
+        out->time = ctx->time;
+        out->Ek = 0.5 * r[0];
+        out->Ep = 0.5 * r[1];
+        for (int k = 0; k < 3; ++k) {
+            out->momentum[k] = r[2 + k];
+            out->angular[k] = r[5 + k];
+        }
+    })
+}
+
+RRG_API rrg_status rrg_calc_mass_center(rrg_ctx* ctx, double center_of_mass[3],
+                                        double* total_mass) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        reduce_state(ctx);
+        const double* r = ctx->host_red;
+        const double M = r[8];
+        for (int k = 0; k < 3; ++k)
+            if (center_of_mass) center_of_mass[k] = M > 0 ? r[9 + k] / M : 0.0;
+        if (total_mass) *total_mass = M;
+    })
+}
+
+// ---------------------------------------------------------------------------------------------
+RRG_API rrg_status rrg_solver_init(rrg_ctx* ctx, const rrg_sim_params* sim) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        RRG_REQUIRE(sim != nullptr, RRG_ERR_INVALID, "NULL sim params");
+        RRG_REQUIRE(std::isfinite(sim->dt_dynamics) && sim->dt_dynamics > 0, RRG_ERR_INVALID,
+                    "dt_dynamics must be positive");
+        ctx->sim = *sim;
+        ctx->wave_mode = sim->use_wave_model != 0;
+        if (ctx->wave_mode) {
+            RRG_REQUIRE(ctx->has_grid, RRG_ERR_STATE,
+                        "No grid info for rect wave integration solver");
+            RRG_REQUIRE(ctx->has_wave, RRG_ERR_STATE,
+                        "No wave params for rect wave integration solver");
+        }
+        for (auto& kv : ctx->graphs)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        ctx->graphs.clear();
+        ctx->solver_ready = true;
+    })
+}
+
+RRG_API rrg_status rrg_solver_precalc(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
+        if (ctx->wave_mode) {
+            deposit_operator(ctx);
+            set_periodic(ctx, 1.0, 0);  // total mass fixed to 1: rrgsim_integration_rect.cuh:65
+            solve_wave(ctx, ctx->wave.setup_iterations, nullptr);
+            gradient(ctx);
+        } else {
+            DirectEpi e;
+            e.mode = EPI_STORE;
+            e.acc = ctx->acc.p;
+            e.pot = ctx->pot.p;
+            direct(ctx, true, e);
+        }
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
+        RRG_REQUIRE(nsteps >= 0, RRG_ERR_INVALID, "nsteps must be >= 0");
+        if (nsteps > 0) {
+            const bool checks_inside =
+                ctx->wave_mode && ctx->wave.steady_check_step > 0 &&
+                ctx->wave.iterations > ctx->wave.steady_check_step;
+            if (checks_inside) {
+                wave_steps_unfused(ctx, nsteps);
+            } else {
+                if (ctx->wave_mode && ctx->src_dirty) {
+                    // keep the invariant "mg[1 - mg_cur] is zero" before the fused steps
+                    RRG_CUDA(cudaMemsetAsync(ctx->mg[1 - ctx->mg_cur].p, 0,
+                                             ctx->mg[1 - ctx->mg_cur].bytes, ctx->stream));
+                }
+                // long runs are recorded once per chunk length and replayed
+                int left = nsteps;
+                while (left > 0) {
+                    const int chunk = std::min(left, 64);
+                    run_graph(ctx, chunk);
+                    left -= chunk;
+                }
+            }
+            for (int s = 0; s < nsteps; ++s) {
+                ctx->iter += 1;
+                ctx->time += ctx->sim.dt_dynamics;
+            }
+        }
+    })
+}
+
+RRG_API rrg_status rrg_solver_sync(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
+        if (ctx->wave_mode) {
+            launch_ngp_phi(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->gdev,
+                           ctx->phi[ctx->phi_cur].p, ctx->pot.p, ctx->stream);
+            launch_interp(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->gdev, ctx->acc4.p,
+                          ctx->acc.p, ctx->stream);
+        } else {
+            ensure_download(ctx, v4b(ctx) * ctx->n);
+            DirectEpi e;
+            e.mode = EPI_STORE;
+            e.acc = ctx->dl.p;
+            e.pot = ctx->pot.p;
+            direct(ctx, true, e);
+        }
+    })
+}
+
+RRG_API rrg_status rrg_set_sort_interval(rrg_ctx* ctx, int interval) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(interval >= 0, RRG_ERR_INVALID, "interval must be >= 0");
+        ctx->sort_interval = interval;
+    })
+}
+
+// ---------------------------------------------------------------------------------------------
+RRG_API rrg_status rrg_dev_direct_forces_f32(const void* posm, const void* poslo,
+                                             const void* hsoft, float uniform_hsoft, int64_t n,
+                                             void* out, int precision, void* stream) {
+    try {
+        RRG_REQUIRE(posm && out && n > 0, RRG_ERR_INVALID, "rrg_dev_direct_forces_f32: bad args");
+        RRG_REQUIRE(precision == RRG_PREC_FP32 || precision == RRG_PREC_MIXED, RRG_ERR_INVALID,
+                    "rrg_dev_direct_forces_f32: precision must be FP32 or MIXED");
+        int dev = 0;
+        RRG_CUDA(cudaGetDevice(&dev));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        DirectLaunch L;
+        L.prec = precision;
+        L.posm = posm;
+        L.poslo = poslo;
+        L.hsoft = hsoft;
+        L.uniform_hsoft = uniform_hsoft;
+        L.n = n;
+        L.want_pot = true;
+        // write (ax, ay, az, phi) into out: acc slot gets a, the potential goes to w through a
+        // strided view is not possible, so compute into out then patch w with the potential
+        L.epi.mode = EPI_STORE;
+        L.epi.acc = out;
+        L.splits = direct_choose_splits(precision, n, num_sms(dev));
+        L.scratch_bytes = direct_scratch_bytes(precision, n, L.splits);
+        void* pot = nullptr;
+        RRG_CUDA(cudaMallocAsync(&pot, sizeof(float) * n + L.scratch_bytes, s));
+        L.epi.pot = pot;
+        L.scratch = L.scratch_bytes ? static_cast<char*>(pot) + sizeof(float) * n : nullptr;
+        L.stream = s;
+        try {
+            launch_direct(L);
+        } catch (...) {
+            cudaFreeAsync(pot, s);
+            throw;
+        }
+        // out[i].w = pot[i]
+        RRG_CUDA(cudaMemcpy2DAsync(static_cast<char*>(out) + 12, 16, pot, 4, 4, n,
+                                   cudaMemcpyDeviceToDevice, s));
+        RRG_CUDA(cudaFreeAsync(pot, s));
+        return RRG_OK;
+    } catch (const Error& e) {
+        t_error = e.what();
+        return e.code;
+    }
+}
+
+RRG_API rrg_status rrg_dev_direct_vjp_f32(const void* posm, const void* hsoft,
+                                          float uniform_hsoft, int64_t n, const void* lam,
+                                          void* out, void* stream) {
+    try {
+        RRG_REQUIRE(posm && lam && out && n > 0, RRG_ERR_INVALID,
+                    "rrg_dev_direct_vjp_f32: bad args");
+        launch_direct_vjp_f32(posm, hsoft, uniform_hsoft, n, lam, out,
+                              static_cast<cudaStream_t>(stream));
+        return RRG_OK;
+    } catch (const Error& e) {
+        t_error = e.what();
+        return e.code;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,286 @@
+// Leapfrog (predict/correct), FP64 diagnostics and state packing on sm_100a.
+#include "kernels.cuh"
+
+namespace rrg {
+namespace {
+
+// predict_step_ (solver/lib/rrgsim_nbody/src/nbody.cu:122-152):
+//   v* = v + dt a ;  x += dt 0.5 (v + v*)
+// The sum v + v* is kept as u so correct_step_ (:159-181) can form 0.5 (v + v* + dt a_new).
+template <typename R, bool MIXED>
+__global__ void predict_kernel(int64_t n, V4<R>* __restrict__ posm, V4<float>* __restrict__ lo,
+                               const V4<R>* __restrict__ vel, const V4<R>* __restrict__ acc,
+                               V4<R>* __restrict__ u, R dt) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V4<R> v = vel[i];
+    const V4<R> a = acc[i];
+    const R sx = v.x + dt * a.x, sy = v.y + dt * a.y, sz = v.z + dt * a.z;
+    const R ux = v.x + sx, uy = v.y + sy, uz = v.z + sz;
+    u[i] = v4<R>(ux, uy, uz, R(0));
+    const R hdt = dt * R(0.5);
+    V4<R> p = posm[i];
+    if constexpr (MIXED) {
+        V4<float> l = lo[i];
+        df_add(p.x, l.x, hdt * ux);
+        df_add(p.y, l.y, hdt * uy);
+        df_add(p.z, l.z, hdt * uz);
+        lo[i] = l;
+    } else {
+        p.x = p.x + hdt * ux;
+        p.y = p.y + hdt * uy;
+        p.z = p.z + hdt * uz;
+    }
+    posm[i] = p;
+}
+
+template <typename R>
+__global__ void correct_kernel(int64_t n, V4<R>* __restrict__ vel, const V4<R>* __restrict__ acc,
+                               const V4<R>* __restrict__ u, R dt) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V4<R> a = acc[i];
+    const V4<R> uu = u[i];
+    vel[i] = v4<R>(R(0.5) * (uu.x + dt * a.x), R(0.5) * (uu.y + dt * a.y),
+                   R(0.5) * (uu.z + dt * a.z), R(0));
+}
+
+// ---------------------------------------------------------------------------------------------
+// FP64 reductions: per particle (promoted to double)
+//   Ek2 += m v^2, Ep2 += m phi, P += m v, L += m (x cross v), M += m, Mx += m x
+// Block partials are summed by one block in a fixed order (deterministic).
+// calc_conservation: nbody.cu:246-291; compute_center_of_mass_kernel: nbody.cu:293-396.
+// ---------------------------------------------------------------------------------------------
+constexpr int kRedThreads = 256;
+constexpr int kRedVals = 12;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename R, bool MIXED>
+__global__ void __launch_bounds__(kRedThreads) conservation_kernel(
+    int64_t n, const V4<R>* __restrict__ posm, const V4<float>* __restrict__ lo,
+    const V4<R>* __restrict__ vel, const R* __restrict__ pot, double* __restrict__ partial) {
+    double acc[kRedVals];
+#pragma unroll
+    for (int k = 0; k < kRedVals; ++k) acc[k] = 0.0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const V4<R> p = posm[i];
+        double x = p.x, y = p.y, z = p.z;
+        if constexpr (MIXED) {
+            const V4<float> l = lo[i];
+            x += l.x;
+            y += l.y;
+            z += l.z;
+        }
+        const double m = p.w;
+        const V4<R> v = vel[i];
+        const double vx = v.x, vy = v.y, vz = v.z;
+        acc[0] += m * (vx * vx + vy * vy + vz * vz);
+        acc[1] += pot ? m * static_cast<double>(pot[i]) : 0.0;
+        acc[2] += m * vx;
+        acc[3] += m * vy;
+        acc[4] += m * vz;
+        acc[5] += m * (vz * y - vy * z);
+        acc[6] += m * (vx * z - vz * x);
+        acc[7] += m * (vy * x - vx * y);
+        acc[8] += m;
+        acc[9] += m * x;
+        acc[10] += m * y;
+        acc[11] += m * z;
+    }
+    __shared__ double s[kRedThreads / 32][kRedVals];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kRedVals; ++k) {
+        const double t = warp_sum(acc[k]);
+        if (lane == 0) s[w][k] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < kRedVals) {
+        double t = 0.0;
+        for (int ww = 0; ww < kRedThreads / 32; ++ww) t += s[ww][threadIdx.x];
+        partial[static_cast<int64_t>(blockIdx.x) * kRedVals + threadIdx.x] = t;
+    }
+}
+
+__global__ void conservation_finish(const double* __restrict__ partial, int nblocks,
+                                    double* __restrict__ out) {
+    const int k = threadIdx.x;
+    if (k >= kRedVals) return;
+    double t = 0.0;
+    for (int b = 0; b < nblocks; ++b) t += partial[static_cast<int64_t>(b) * kRedVals + k];
+    out[k] = t;
+}
+
+// Host FP64 AoS -> device state.
+template <typename R, bool MIXED>
+__global__ void pack_kernel(int64_t n, const double* __restrict__ pos3,
+                            const double* __restrict__ vel3, const double* __restrict__ mass,
+                            const double* __restrict__ soft2, V4<R>* __restrict__ posm,
+                            V4<float>* __restrict__ lo, V4<R>* __restrict__ vel,
+                            R* __restrict__ hsoft) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = pos3[3 * i], y = pos3[3 * i + 1], z = pos3[3 * i + 2];
+    posm[i] = v4<R>(static_cast<R>(x), static_cast<R>(y), static_cast<R>(z),
+                    static_cast<R>(mass[i]));
+    if constexpr (MIXED) {
+        const float hx = static_cast<float>(x), hy = static_cast<float>(y),
+                    hz = static_cast<float>(z);
+        lo[i] = v4<float>(static_cast<float>(x - hx), static_cast<float>(y - hy),
+                          static_cast<float>(z - hz), 0.f);
+    }
+    vel[i] = v4<R>(static_cast<R>(vel3[3 * i]), static_cast<R>(vel3[3 * i + 1]),
+                   static_cast<R>(vel3[3 * i + 2]), R(0));
+    if (hsoft) hsoft[i] = static_cast<R>(0.5 * soft2[i]);
+}
+
+template <typename R, bool MIXED>
+__global__ void unpack_kernel(int64_t n, const int32_t* __restrict__ id,
+                              const V4<R>* __restrict__ posm, const V4<float>* __restrict__ lo,
+                              const V4<R>* __restrict__ vel, const V4<R>* __restrict__ acc,
+                              const R* __restrict__ pot, double* __restrict__ pos3,
+                              double* __restrict__ vel3, double* __restrict__ acc3,
+                              double* __restrict__ grav) {
+    const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t i = id ? static_cast<int64_t>(id[s]) : s;
+    if (pos3) {
+        const V4<R> p = posm[s];
+        double x = p.x, y = p.y, z = p.z;
+        if constexpr (MIXED) {
+            const V4<float> l = lo[s];
+            x += l.x;
+            y += l.y;
+            z += l.z;
+        }
+        pos3[3 * i] = x;
+        pos3[3 * i + 1] = y;
+        pos3[3 * i + 2] = z;
+    }
+    if (vel3) {
+        const V4<R> v = vel[s];
+        vel3[3 * i] = v.x;
+        vel3[3 * i + 1] = v.y;
+        vel3[3 * i + 2] = v.z;
+    }
+    if (acc3) {
+        const V4<R> a = acc[s];
+        acc3[3 * i] = a.x;
+        acc3[3 * i + 1] = a.y;
+        acc3[3 * i + 2] = a.z;
+    }
+    if (grav) grav[i] = pot[s];
+}
+
+}  // namespace
+
+void launch_predict(int prec, int64_t n, void* posm, void* poslo, const void* vel,
+                    const void* acc, void* u, double dt, cudaStream_t s) {
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        predict_kernel<double, false><<<b, 256, 0, s>>>(
+            n, static_cast<V4<double>*>(posm), nullptr, static_cast<const V4<double>*>(vel),
+            static_cast<const V4<double>*>(acc), static_cast<V4<double>*>(u), dt);
+    else if (prec == RRG_PREC_MIXED)
+        predict_kernel<float, true><<<b, 256, 0, s>>>(
+            n, static_cast<V4<float>*>(posm), static_cast<V4<float>*>(poslo),
+            static_cast<const V4<float>*>(vel), static_cast<const V4<float>*>(acc),
+            static_cast<V4<float>*>(u), static_cast<float>(dt));
+    else
+        predict_kernel<float, false><<<b, 256, 0, s>>>(
+            n, static_cast<V4<float>*>(posm), nullptr, static_cast<const V4<float>*>(vel),
+            static_cast<const V4<float>*>(acc), static_cast<V4<float>*>(u),
+            static_cast<float>(dt));
+    RRG_LAUNCHED();
+}
+
+void launch_correct(int prec, int64_t n, void* vel, const void* acc, const void* u, double dt,
+                    cudaStream_t s) {
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        correct_kernel<double><<<b, 256, 0, s>>>(n, static_cast<V4<double>*>(vel),
+                                                 static_cast<const V4<double>*>(acc),
+                                                 static_cast<const V4<double>*>(u), dt);
+    else
+        correct_kernel<float><<<b, 256, 0, s>>>(n, static_cast<V4<float>*>(vel),
+                                                static_cast<const V4<float>*>(acc),
+                                                static_cast<const V4<float>*>(u),
+                                                static_cast<float>(dt));
+    RRG_LAUNCHED();
+}
+
+int conservation_blocks(int64_t n) {
+    const int b = div_up(n, kRedThreads);
+    return b < 1184 ? (b < 1 ? 1 : b) : 1184;
+}
+
+void launch_conservation(int prec, int64_t n, const void* posm, const void* poslo,
+                         const void* vel, const void* pot, double* partial, int nblocks,
+                         double* out, cudaStream_t s) {
+    if (prec == RRG_PREC_FP64)
+        conservation_kernel<double, false><<<nblocks, kRedThreads, 0, s>>>(
+            n, static_cast<const V4<double>*>(posm), nullptr,
+            static_cast<const V4<double>*>(vel), static_cast<const double*>(pot), partial);
+    else if (prec == RRG_PREC_MIXED)
+        conservation_kernel<float, true><<<nblocks, kRedThreads, 0, s>>>(
+            n, static_cast<const V4<float>*>(posm), static_cast<const V4<float>*>(poslo),
+            static_cast<const V4<float>*>(vel), static_cast<const float*>(pot), partial);
+    else
+        conservation_kernel<float, false><<<nblocks, kRedThreads, 0, s>>>(
+            n, static_cast<const V4<float>*>(posm), nullptr, static_cast<const V4<float>*>(vel),
+            static_cast<const float*>(pot), partial);
+    RRG_LAUNCHED();
+    conservation_finish<<<1, 32, 0, s>>>(partial, nblocks, out);
+    RRG_LAUNCHED();
+}
+
+void launch_pack_state(int prec, int64_t n, const double* pos3, const double* vel3,
+                       const double* mass, const double* soft2, void* posm, void* poslo,
+                       void* vel, void* hsoft, cudaStream_t s) {
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        pack_kernel<double, false><<<b, 256, 0, s>>>(
+            n, pos3, vel3, mass, soft2, static_cast<V4<double>*>(posm), nullptr,
+            static_cast<V4<double>*>(vel), static_cast<double*>(hsoft));
+    else if (prec == RRG_PREC_MIXED)
+        pack_kernel<float, true><<<b, 256, 0, s>>>(
+            n, pos3, vel3, mass, soft2, static_cast<V4<float>*>(posm),
+            static_cast<V4<float>*>(poslo), static_cast<V4<float>*>(vel),
+            static_cast<float*>(hsoft));
+    else
+        pack_kernel<float, false><<<b, 256, 0, s>>>(
+            n, pos3, vel3, mass, soft2, static_cast<V4<float>*>(posm), nullptr,
+            static_cast<V4<float>*>(vel), static_cast<float*>(hsoft));
+    RRG_LAUNCHED();
+}
+
+void launch_unpack_state(int prec, int64_t n, const int32_t* id, const void* posm,
+                         const void* poslo, const void* vel, const void* acc, const void* pot,
+                         double* pos3, double* vel3, double* acc3, double* grav,
+                         cudaStream_t s) {
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        unpack_kernel<double, false><<<b, 256, 0, s>>>(
+            n, id, static_cast<const V4<double>*>(posm), nullptr,
+            static_cast<const V4<double>*>(vel), static_cast<const V4<double>*>(acc),
+            static_cast<const double*>(pot), pos3, vel3, acc3, grav);
+    else if (prec == RRG_PREC_MIXED)
+        unpack_kernel<float, true><<<b, 256, 0, s>>>(
+            n, id, static_cast<const V4<float>*>(posm), static_cast<const V4<float>*>(poslo),
+            static_cast<const V4<float>*>(vel), static_cast<const V4<float>*>(acc),
+            static_cast<const float*>(pot), pos3, vel3, acc3, grav);
+    else
+        unpack_kernel<float, false><<<b, 256, 0, s>>>(
+            n, id, static_cast<const V4<float>*>(posm), nullptr,
+            static_cast<const V4<float>*>(vel), static_cast<const V4<float>*>(acc),
+            static_cast<const float*>(pot), pos3, vel3, acc3, grav);
+    RRG_LAUNCHED();
+}
+
+}  // namespace rrg

@@ -1,0 +1,156 @@
+// Launchers of the sm_100a kernels (implemented in direct.cu, pm.cu, integrate.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace rrg {
+
+// ---------------------------------------------------------------------------------------------
+// Direct-sum gravity (nbody.cu:19-114): a_i = sum_j m_j d_ij (|d_ij|^2 + h_i + h_j)^-3/2,
+// phi_i = -sum_j m_j (|d_ij|^2 + h_i + h_j)^-1/2, h = soft2 / 2, self pair included.
+// ---------------------------------------------------------------------------------------------
+enum DirectEpiMode {
+    EPI_STORE = 0,            // acc[i] = a (and pot[i] = phi when requested)
+    EPI_CORRECT = 1,          // v = (u + dt a) / 2 -> vel; acc[i] = a
+    EPI_CORRECT_PREDICT = 2,  // v as above, then u' = v + (v + dt a), x' = x + dt/2 u' -> pos_out
+};
+
+struct DirectEpi {
+    int mode = EPI_STORE;
+    double dt = 0.0;
+    void* acc = nullptr;      // V4<R> (ax, ay, az, 0)
+    void* pot = nullptr;      // R[n]
+    void* vel = nullptr;      // V4<R>
+    void* u = nullptr;        // V4<R> holding v + v* (the reference's vel + vel_predicted_)
+    void* pos_out = nullptr;  // V4<R> (x, y, z, m) after the drift
+    void* lo_out = nullptr;   // V4<float> low parts after the drift (MIXED)
+};
+
+struct DirectLaunch {
+    int prec = RRG_PREC_FP32;
+    const void* posm = nullptr;   // V4<R> (x, y, z, m); for MIXED the hi parts
+    const void* poslo = nullptr;  // V4<float> (MIXED only)
+    const void* hsoft = nullptr;  // R[n] soft2/2, or nullptr -> uniform_hsoft
+    double uniform_hsoft = 0.0;
+    int64_t n = 0;
+    bool want_pot = false;
+    DirectEpi epi;
+    int splits = 0;               // j-splits; 0 = choose
+    void* scratch = nullptr;      // partial sums when splits > 1
+    size_t scratch_bytes = 0;
+    cudaStream_t stream = nullptr;
+};
+
+int direct_choose_splits(int prec, int64_t n, int sms);
+size_t direct_scratch_bytes(int prec, int64_t n, int splits);
+void launch_direct(const DirectLaunch& L);
+
+// VJP of a(x, m) (FP32): out_i = (d<lam,a>/dx_i, d<lam,a>/dm_i).
+void launch_direct_vjp_f32(const void* posm, const void* hsoft, float uniform_hsoft, int64_t n,
+                           const void* lam, void* out, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------------------------
+// Leapfrog pieces (nbody.cu:122-181) on the context state.
+// ---------------------------------------------------------------------------------------------
+// v* = v + dt a; u = v + v*; x += dt/2 u   (MIXED: x kept as hi + lo)
+void launch_predict(int prec, int64_t n, void* posm, void* poslo, const void* vel,
+                    const void* acc, void* u, double dt, cudaStream_t s);
+// v = (u + dt a) / 2
+void launch_correct(int prec, int64_t n, void* vel, const void* acc, const void* u, double dt,
+                    cudaStream_t s);
+
+// FP64 reductions of the state (calc_conservation, nbody.cu:246-291; centre of mass,
+// nbody.cu:293-439). out[0..11] = Ek2 (sum m v^2), Ep2 (sum m phi), P[3], L[3], M, Mx[3].
+void launch_conservation(int prec, int64_t n, const void* posm, const void* poslo,
+                         const void* vel, const void* pot, double* partial, int nblocks,
+                         double* out, cudaStream_t s);
+int conservation_blocks(int64_t n);
+
+// Conversions between the host FP64 AoS layout and the device state.
+void launch_pack_state(int prec, int64_t n, const double* pos3, const double* vel3,
+                       const double* mass, const double* soft2, void* posm, void* poslo,
+                       void* vel, void* hsoft, cudaStream_t s);
+// Gathers back into the original order through id (sorted slot -> original index).
+void launch_unpack_state(int prec, int64_t n, const int32_t* id, const void* posm,
+                         const void* poslo, const void* vel, const void* acc, const void* pot,
+                         double* pos3, double* vel3, double* acc3, double* grav,
+                         cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Particle-mesh (rm_p2mesh.cu, rm_mesh2p.cu, wave.cu)
+// ---------------------------------------------------------------------------------------------
+struct WaveCoef {
+    // per-cell coefficients are uniform unless the dissipation layer is on
+    double K_MAIN, K_ACTUAL, K_OLD, K_F;
+    // for the non-uniform case (layer dissipation or non-periodic boundaries)
+    double C, DT, DX, diss_base, diss_extra, sim_l, domain_min;
+    int bc_type;
+    int keep_layer;
+    double rho_mean;
+    double bc_mass, com[3], r_min;
+};
+
+// CIC deposit into int64 fixed point (rm_p2mesh.cu:176-236): cell += round(m w 2^S).
+void launch_cic_deposit(int prec, int64_t n, const void* posm, const void* poslo,
+                        const GridDev& g, int shift_s, unsigned long long* grid,
+                        cudaStream_t s);
+// Wave source from the fixed-point mass: src = 4 pi G (m 2^-S / dx^3 - rho_mean) [* K_F when
+// uniform], stored in R; optionally zeroes the fixed-point grid.
+void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int shift_s,
+                        double dx, double rho_mean, double scale, void* src, bool zero_grid,
+                        cudaStream_t s);
+// One damped-wave substep (wave.cu:106-193): phi_old_inout <- phi_new.
+// If maxbits != nullptr also folds max|phi_new - phi| and max|phi_new| into maxbits[0..1].
+void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, const void* src,
+                      const WaveCoef& c, unsigned long long* maxbits, cudaStream_t s);
+// a = -grad phi on the grid (rm_p2mesh.cu:238-290): acc4[c] = (ax, ay, az, phi[c]).
+void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, cudaStream_t s);
+// Trilinear gather of acc4 to particles (rm_mesh2p.cu:48-114).
+void launch_interp(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
+                   const void* acc4, void* acc, cudaStream_t s);
+// NGP potential lookup (rm_mesh2p.cu:29-38 with the cell of rm_p2mesh.cu:25-49).
+void launch_ngp_phi(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
+                    const void* phi, void* pot, cudaStream_t s);
+
+// Fused particle pass of the wave strategy: optional [trilinear interp + correct] then
+// optional [predict + CIC deposit].
+enum PmMode { PM_INTERP_CORRECT = 1, PM_PREDICT_DEPOSIT = 2, PM_WRITE_SYNC = 4 };
+struct PmParticleArgs {
+    int prec;
+    int64_t n;
+    void* posm;
+    void* poslo;
+    void* vel;    // V4<R> synced velocity (read when !INTERP_CORRECT, written when WRITE_SYNC)
+    void* acc;    // V4<R> synced acceleration (same rules)
+    void* u;      // V4<R>
+    const void* acc4;  // grid field
+    GridDev g;
+    int shift_s;
+    unsigned long long* mgrid;
+    double dt;
+};
+void launch_pm_particles(const PmParticleArgs& a, int mode, cudaStream_t s);
+
+// Counting sort by NGP cell: keys, histogram, scan, scatter of the particle arrays.
+struct SortArgs {
+    int prec;
+    int64_t n;
+    GridDev g;
+    // arrays permuted (in -> out); any may be nullptr
+    const void* posm; void* posm_out;
+    const void* poslo; void* poslo_out;
+    const void* vel; void* vel_out;
+    const void* acc; void* acc_out;
+    const void* u; void* u_out;
+    const void* hsoft; void* hsoft_out;
+    const int32_t* id; int32_t* id_out;
+    // scratch
+    uint32_t* keys;      // n
+    uint32_t* counts;    // nx^3 + 1
+    uint32_t* offsets;   // nx^3 + 1
+    uint32_t* block_sums;  // scan block partials
+};
+size_t sort_scan_blocks(int ncells);
+void launch_sort_by_cell(const SortArgs& a, cudaStream_t s);
+
+}  // namespace rrg

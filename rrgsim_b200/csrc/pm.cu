@@ -1,0 +1,669 @@
+// Particle-mesh kernels on sm_100a: CIC deposit into int64 fixed point, damped-wave potential
+// relaxation, gradient, trilinear force interpolation, and the fused particle pass.
+//
+// Grid layout is the reference's AT(x, y, z) = x + y nx + z nx^2
+// (solver/lib/rrgsim_common/include/co_device_utils.cuh:61), nx^3 cells, cell centres at
+// domain_min + (i + 1/2) dx for CIC / interpolation and nodes at domain_min + i dx for the wave
+// boundary terms (wave.cu:18-20), exactly as in the reference.
+#include "kernels.cuh"
+
+namespace rrg {
+namespace {
+
+constexpr double kPi = 3.14159265358979;  // the reference's PI (co_info_structs.h:7)
+
+__device__ __forceinline__ int wrap_mod(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+__device__ __forceinline__ double load_x(const V4<float>* posm, const V4<float>* lo, int64_t i,
+                                         double& y, double& z, float& m) {
+    const V4<float> p = posm[i];
+    double x = p.x;
+    y = p.y;
+    z = p.z;
+    if (lo) {
+        const V4<float> l = lo[i];
+        x += l.x;
+        y += l.y;
+        z += l.z;
+    }
+    m = p.w;
+    return x;
+}
+
+// ----------------------------------------------------------------------------------------------
+// CIC weights exactly as deposit_cell_mass_CIC_ (rm_p2mesh.cu:184-226), in FP64 with every
+// operation rounded separately (no FMA contraction) so that the host oracle, compiled with
+// -ffp-contract=off, produces the same bits:
+//   u = (x - domain_min) * inv_dx - 0.5 ; clamp to [0, nx - 1 - 1e-6]
+//   i0 = floor(u) ; i1 = min(i0 + 1, nx - 1) ; f = u - i0 ; w0 = 1 - f ; w1 = f
+// A NaN coordinate is treated as u = 0 (the reference would index out of bounds).
+// ----------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cic_axis(double x, double dmin, double inv_dx, int nx, int& i0,
+                                         int& i1, double& w0, double& w1) {
+    double u = __dsub_rn(__dmul_rn(__dsub_rn(x, dmin), inv_dx), 0.5);
+    const double hi = __dsub_rn(static_cast<double>(nx - 1), 1e-6);
+    if (!(u >= 0.0)) u = 0.0;  // also catches NaN
+    if (u > hi) u = hi;
+    i0 = static_cast<int>(floor(u));
+    i1 = min(i0 + 1, nx - 1);
+    const double f = __dsub_rn(u, static_cast<double>(i0));
+    w0 = __dsub_rn(1.0, f);
+    w1 = f;
+}
+
+// Deposits one particle (all lanes of the warp call this together, converged).
+// Lanes with the same base cell form a group (__match_any_sync); each of the 8 corner values
+// is summed over the group with one redux.sync and added by the group leader with one 64-bit
+// atomic. Values fit in 27 bits (the scale S is chosen so that m_max 2^S <= 2^26), so a warp
+// sum fits the 32-bit redux.
+__device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y, double z,
+                                                 double m, const GridDev& g, double scale,
+                                                 unsigned long long* __restrict__ grid) {
+    const int nx = g.nx;
+    int i0 = 0, i1 = 0, j0 = 0, j1 = 0, k0 = 0, k1 = 0;
+    double wx0 = 0, wx1 = 0, wy0 = 0, wy1 = 0, wz0 = 0, wz1 = 0;
+    if (active) {
+        cic_axis(x, g.domain_min, g.inv_dx, nx, i0, i1, wx0, wx1);
+        cic_axis(y, g.domain_min, g.inv_dx, nx, j0, j1, wy0, wy1);
+        cic_axis(z, g.domain_min, g.inv_dx, nx, k0, k1, wz0, wz1);
+    }
+    const int64_t nx2 = static_cast<int64_t>(nx) * nx;
+    const int base = active ? (i0 + j0 * nx + k0 * static_cast<int>(nx2)) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, base);
+    const bool leader = (threadIdx.x & 31) == (__ffs(peers) - 1);
+    const double ms = __dmul_rn(m, scale);
+    // corner order and weight products as rm_p2mesh.cu:219-235
+    const int ii[8] = {i0, i1, i0, i1, i0, i1, i0, i1};
+    const int jj[8] = {j0, j0, j1, j1, j0, j0, j1, j1};
+    const int kk[8] = {k0, k0, k0, k0, k1, k1, k1, k1};
+    const double wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        unsigned q = 0;
+        if (active) {
+            const double w = __dmul_rn(__dmul_rn(wxs[c & 1], wys[(c >> 1) & 1]), wzs[c >> 2]);
+            q = static_cast<unsigned>(__double2ll_rn(__dmul_rn(ms, w)));
+        }
+        const unsigned s = __reduce_add_sync(peers, q);
+        if (active && leader && s != 0u) {
+            const int64_t a = ii[c] + static_cast<int64_t>(jj[c]) * nx + kk[c] * nx2;
+            atomicAdd(grid + a, static_cast<unsigned long long>(s));
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void load_pos(const void* posm, const V4<float>* lo, int64_t i,
+                                         double& x, double& y, double& z, double& m) {
+    if constexpr (sizeof(R) == 8) {
+        const V4<double> p = static_cast<const V4<double>*>(posm)[i];
+        x = p.x;
+        y = p.y;
+        z = p.z;
+        m = p.w;
+    } else {
+        float mf;
+        x = load_x(static_cast<const V4<float>*>(posm), lo, i, y, z, mf);
+        m = mf;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) cic_kernel(int64_t n, const void* __restrict__ posm,
+                                                  const V4<float>* __restrict__ lo, GridDev g,
+                                                  double scale,
+                                                  unsigned long long* __restrict__ grid) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    double x = 0, y = 0, z = 0, m = 0;
+    if (active) load_pos<R>(posm, lo, i, x, y, z, m);
+    cic_deposit_warp(active, x, y, z, m, g, scale, grid);
+}
+
+// ----------------------------------------------------------------------------------------------
+// Wave source: f = 4 pi G rho, rho = mass / dx^3 - rho_sub (wave.cu:150-153), mass from the
+// fixed-point grid. Optionally clears the fixed-point grid for the next deposit.
+// ----------------------------------------------------------------------------------------------
+template <typename R>
+__global__ void wave_source_kernel(int64_t ncells, unsigned long long* __restrict__ mgrid,
+                                   double inv_scale, double dx, double rho_sub, double mult,
+                                   R* __restrict__ src, bool zero_grid) {
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    const unsigned long long q = mgrid[c];
+    if (zero_grid) mgrid[c] = 0ull;
+    const double mass = static_cast<double>(q) * inv_scale;
+    const double rho = mass / (dx * dx * dx) - rho_sub;
+    src[c] = static_cast<R>(mult * (4.0 * kPi * 1.0 * rho));
+}
+
+// ----------------------------------------------------------------------------------------------
+// Damped wave substep (wave_diss_iteration, wave.cu:106-193).
+//   phi_new = K_MAIN sum6 + K_ACTUAL phi + K_OLD phi_old + K_F f
+// 2.5D blocking: a 32 x 8 (x, y) tile of threads marches through zc z-planes; the current plane
+// sits in shared memory with a one-cell halo, the z-neighbours in registers, so phi is read
+// about once per cell. phi_new overwrites phi_old in place (each cell's old value is read only
+// by its own thread), so two grid buffers rotate instead of the reference's three.
+// ----------------------------------------------------------------------------------------------
+constexpr int kTX = 32, kTY = 8;
+
+struct WaveDev {
+    int nx;
+    int zc;
+    int bc;          // rrg_boundary_type
+    int uniform;     // periodic without absorbing layer -> constant coefficients
+    double K_MAIN, K_ACTUAL, K_OLD, K_F;
+    double C, DT, DX, diss_base, diss_extra, sim_l, domain_min;
+    double bc_mass, comx, comy, comz, r_min;
+};
+
+__device__ __forceinline__ double layer_diss(const WaveDev& w, double x) {
+    const double x_in = 0.5 * w.sim_l;
+    const double d = fabs(x) - x_in;
+    return d > 0 ? w.diss_extra * d * d : 0.0;
+}
+
+__device__ __forceinline__ double monopole_phi(const WaveDev& w, double x, double y, double z) {
+    const double rx = w.comx - x, ry = w.comy - y, rz = w.comz - z;
+    const double dist = sqrt(rx * rx + ry * ry + rz * rz);
+    const double r = fmax(dist, w.r_min);
+    return -1.0 * w.bc_mass / r;
+}
+
+template <typename R>
+__device__ __forceinline__ double psi_at(const WaveDev& w, const R* phi, int i, int j, int k) {
+    const int64_t nx = w.nx;
+    const double x = w.domain_min + i * w.DX, y = w.domain_min + j * w.DX,
+                 z = w.domain_min + k * w.DX;
+    return static_cast<double>(phi[i + j * nx + k * nx * nx]) - monopole_phi(w, x, y, z);
+}
+
+// Radiative boundary node (radiative_boundary / upwind_axis, wave.cu:51-104).
+template <typename R>
+__device__ double radiative_value(const WaveDev& w, const R* phi, int ix, int iy, int iz) {
+    const double x = w.domain_min + ix * w.DX, y = w.domain_min + iy * w.DX,
+                 z = w.domain_min + iz * w.DX;
+    const double rx = x - w.comx, ry = y - w.comy, rz = z - w.comz;
+    const double r = fmax(sqrt(rx * rx + ry * ry + rz * rz), w.r_min);
+    const double n3[3] = {rx / r, ry / r, rz / r};
+    const double psi0 = psi_at<R>(w, phi, ix, iy, iz);
+    double dpsi_dr = 0.0;
+    const int idx[3] = {ix, iy, iz};
+    for (int axis = 0; axis < 3; ++axis) {
+        const int i0 = idx[axis];
+        int in = (n3[axis] > 0) ? i0 - 1 : i0 + 1;
+        if (in < 0 || in >= w.nx) in = 2 * i0 - in;
+        int jx = ix, jy = iy, jz = iz;
+        if (axis == 0) jx = in;
+        else if (axis == 1) jy = in;
+        else jz = in;
+        const double d = (psi0 - psi_at<R>(w, phi, jx, jy, jz)) / ((i0 - in) * w.DX);
+        dpsi_dr += n3[axis] * d;
+    }
+    const double psi_new = psi0 - w.C * w.DT * (dpsi_dr + psi0 / r);
+    return psi_new + monopole_phi(w, x, y, z);
+}
+
+__device__ __forceinline__ unsigned long long dbits(double v) {
+    return static_cast<unsigned long long>(__double_as_longlong(v));
+}
+
+template <typename R, bool UNIFORM, bool CHECK>
+__global__ void __launch_bounds__(kTX* kTY) wave_step_kernel(
+    const R* __restrict__ phi, R* __restrict__ phi_old, const R* __restrict__ src,
+    const WaveDev w, unsigned long long* __restrict__ maxbits) {
+    __shared__ R tile[kTY + 2][kTX + 2];
+    const int nx = w.nx;
+    const int64_t nx2 = static_cast<int64_t>(nx) * nx;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * kTX + tx;
+    const int x = blockIdx.x * kTX + tx;
+    const int y = blockIdx.y * kTY + ty;
+    const bool valid = (x < nx) && (y < nx);
+    const bool periodic = (w.bc == RRG_BC_PERIODIC);
+    // coordinates used for loads: wrapped (periodic) or clamped (others; values then unused)
+    const int xl = periodic ? wrap_mod(x, nx) : min(x, nx - 1);
+    const int yl = periodic ? wrap_mod(y, nx) : min(y, nx - 1);
+    const int z0 = blockIdx.z * w.zc;
+    const int z1 = min(nx, z0 + w.zc);
+
+    // halo cell handled by this thread (80 halo cells: two rows of 32, two columns of 8)
+    int hsx = -1, hsy = -1, hgx = 0, hgy = 0;
+    if (tid < 2 * kTX + 2 * kTY) {
+        if (tid < kTX) { hsx = tid + 1; hsy = 0; }
+        else if (tid < 2 * kTX) { hsx = tid - kTX + 1; hsy = kTY + 1; }
+        else if (tid < 2 * kTX + kTY) { hsx = 0; hsy = tid - 2 * kTX + 1; }
+        else { hsx = kTX + 1; hsy = tid - 2 * kTX - kTY + 1; }
+        const int gx = blockIdx.x * kTX + hsx - 1;
+        const int gy = blockIdx.y * kTY + hsy - 1;
+        hgx = periodic ? wrap_mod(gx, nx) : max(0, min(gx, nx - 1));
+        hgy = periodic ? wrap_mod(gy, nx) : max(0, min(gy, nx - 1));
+    }
+
+    auto zidx = [&](int z) -> int64_t {
+        const int zz = periodic ? wrap_mod(z, nx) : max(0, min(z, nx - 1));
+        return zz * nx2;
+    };
+    const int64_t col = xl + static_cast<int64_t>(yl) * nx;
+    R pm = phi[col + zidx(z0 - 1)];
+    R pc = phi[col + zidx(z0)];
+
+    double dmax = 0.0, amax = 0.0;
+    for (int z = z0; z < z1; ++z) {
+        const R pn = phi[col + zidx(z + 1)];
+        R hval = R(0);
+        if (hsx >= 0) hval = phi[hgx + static_cast<int64_t>(hgy) * nx + zidx(z)];
+        __syncthreads();
+        tile[ty + 1][tx + 1] = pc;
+        if (hsx >= 0) tile[hsy][hsx] = hval;
+        __syncthreads();
+        if (valid) {
+            const int64_t c = x + static_cast<int64_t>(y) * nx + z * nx2;
+            const bool on_edge = x == 0 || x == nx - 1 || y == 0 || y == nx - 1 || z == 0 ||
+                                 z == nx - 1;
+            R out;
+            if (!periodic && on_edge) {
+                double v = 0.0;
+                if (w.bc == RRG_BC_MONOPOLE_DIRICHLET)
+                    v = monopole_phi(w, w.domain_min + x * w.DX, w.domain_min + y * w.DX,
+                                     w.domain_min + z * w.DX);
+                else if (w.bc == RRG_BC_MONOPOLE_RADIATIVE)
+                    v = radiative_value<R>(w, phi, x, y, z);
+                out = static_cast<R>(v);
+            } else {
+                const R lap = tile[ty + 1][tx] + tile[ty + 1][tx + 2] + tile[ty][tx + 1] +
+                              tile[ty + 2][tx + 1] + pm + pn;
+                R kmain, kact, kold, kf;
+                if constexpr (UNIFORM) {
+                    kmain = static_cast<R>(w.K_MAIN);
+                    kact = static_cast<R>(w.K_ACTUAL);
+                    kold = static_cast<R>(w.K_OLD);
+                    kf = static_cast<R>(w.K_F);
+                } else {
+                    double diss = w.diss_base;
+                    diss += layer_diss(w, w.domain_min + x * w.DX);
+                    diss += layer_diss(w, w.domain_min + y * w.DX);
+                    diss += layer_diss(w, w.domain_min + z * w.DX);
+                    const double Q = diss * w.C * w.DT * 0.5;
+                    const double W = 1 + Q;
+                    const double K = w.C * w.C * w.DT * w.DT / (w.DX * w.DX);
+                    kmain = static_cast<R>(K / W);
+                    kf = static_cast<R>(-w.C * w.C * w.DT * w.DT / W);
+                    kact = static_cast<R>(2 * (1 - 3 * K) / W);
+                    kold = static_cast<R>((Q - 1) / W);
+                }
+                out = lap * kmain + pc * kact + phi_old[c] * kold + src[c] * kf;
+            }
+            phi_old[c] = out;
+            if constexpr (CHECK) {
+                dmax = fmax(dmax, fabs(static_cast<double>(out) - static_cast<double>(pc)));
+                amax = fmax(amax, fabs(static_cast<double>(out)));
+            }
+        }
+        pm = pc;
+        pc = pn;
+    }
+    if constexpr (CHECK) {
+        // warp max -> block max -> one atomicMax per block on the (non-negative) double bits
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, o));
+            amax = fmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+        }
+        __shared__ double sd[kTX * kTY / 32], sa[kTX * kTY / 32];
+        const int lane = tid & 31, wid = tid >> 5;
+        if (lane == 0) {
+            sd[wid] = dmax;
+            sa[wid] = amax;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double d = 0, a = 0;
+            for (int k = 0; k < kTX * kTY / 32; ++k) {
+                d = fmax(d, sd[k]);
+                a = fmax(a, sa[k]);
+            }
+            atomicMax(maxbits, dbits(d));
+            atomicMax(maxbits + 1, dbits(a));
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Gradient (calc_acceleration_field_, rm_p2mesh.cu:238-290): central differences inside,
+// one-sided at the faces, a = -dphi / dx. Output cell (ax, ay, az, phi).
+// ----------------------------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(kTX* kTY) gradient_kernel(int nx, R coef,
+                                                            const R* __restrict__ phi,
+                                                            V4<R>* __restrict__ acc4) {
+    const int x = blockIdx.x * kTX + threadIdx.x;
+    const int y = blockIdx.y * kTY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= nx) return;
+    const int64_t sx = 1, sy = nx, sz = static_cast<int64_t>(nx) * nx;
+    const int64_t c = x + y * sy + z * sz;
+    const R pc = phi[c];
+    R dx, dy, dz;
+    if (x == 0) dx = phi[c + sx] - pc;
+    else if (x == nx - 1) dx = pc - phi[c - sx];
+    else dx = R(0.5) * (phi[c + sx] - phi[c - sx]);
+    if (y == 0) dy = phi[c + sy] - pc;
+    else if (y == nx - 1) dy = pc - phi[c - sy];
+    else dy = R(0.5) * (phi[c + sy] - phi[c - sy]);
+    if (z == 0) dz = phi[c + sz] - pc;
+    else if (z == nx - 1) dz = pc - phi[c - sz];
+    else dz = R(0.5) * (phi[c + sz] - phi[c - sz]);
+    acc4[c] = v4<R>(dx * coef, dy * coef, dz * coef, pc);
+}
+
+// ----------------------------------------------------------------------------------------------
+// Trilinear gather (interpolate_acceleration_to_particles_kernel, rm_mesh2p.cu:48-114).
+// Index selection as the reference: f = (x - domain_min) / dx - 0.5 in FP64, i0 = floorf(f)
+// (the reference passes its double to floorf, i.e. floors the float-rounded value), weights
+// from the unclamped fraction, indices clamped to [0, nx - 1]; summation order z, y, x.
+// ----------------------------------------------------------------------------------------------
+__device__ __forceinline__ void interp_axis(double x, double dmin, double dx, int nx, int& i0,
+                                            int& i1, double& w) {
+    const double f = (x - dmin) / dx - 0.5;
+    int a = static_cast<int>(floorf(static_cast<float>(f)));
+    w = f - a;
+    i0 = max(0, min(a, nx - 1));
+    i1 = max(0, min(a + 1, nx - 1));
+}
+
+template <typename R>
+__device__ __forceinline__ void trilinear(const V4<R>* __restrict__ acc4, const GridDev& g,
+                                          double x, double y, double z, R& ax, R& ay, R& az) {
+    int i0, i1, j0, j1, k0, k1;
+    double wxd, wyd, wzd;
+    interp_axis(x, g.domain_min, g.dx, g.nx, i0, i1, wxd);
+    interp_axis(y, g.domain_min, g.dx, g.nx, j0, j1, wyd);
+    interp_axis(z, g.domain_min, g.dx, g.nx, k0, k1, wzd);
+    const R wx = static_cast<R>(wxd), wy = static_cast<R>(wyd), wz = static_cast<R>(wzd);
+    const int64_t nx = g.nx;
+    ax = ay = az = R(0);
+#pragma unroll
+    for (int k = 0; k <= 1; ++k) {
+        const int64_t kk = k == 0 ? k0 : k1;
+        const R wk = k == 0 ? (R(1) - wz) : wz;
+#pragma unroll
+        for (int j = 0; j <= 1; ++j) {
+            const int64_t jj = j == 0 ? j0 : j1;
+            const R wj = j == 0 ? (R(1) - wy) : wy;
+#pragma unroll
+            for (int i = 0; i <= 1; ++i) {
+                const int64_t ii = i == 0 ? i0 : i1;
+                const R wi = i == 0 ? (R(1) - wx) : wx;
+                const R weight = wi * wj * wk;
+                const V4<R> f = acc4[kk * nx * nx + jj * nx + ii];
+                ax += weight * f.x;
+                ay += weight * f.y;
+                az += weight * f.z;
+            }
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) interp_kernel(int64_t n, const void* __restrict__ posm,
+                                                     const V4<float>* __restrict__ lo, GridDev g,
+                                                     const V4<R>* __restrict__ acc4,
+                                                     V4<R>* __restrict__ acc) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x, y, z, m;
+    load_pos<R>(posm, lo, i, x, y, z, m);
+    R ax, ay, az;
+    trilinear<R>(acc4, g, x, y, z, ax, ay, az);
+    acc[i] = v4<R>(ax, ay, az, R(0));
+}
+
+// NGP cell as assign_particles_to_cells_ (rm_p2mesh.cu:37-49): truncation, clamp.
+__device__ __forceinline__ int ngp_axis(double x, double dmin, double dx, int nx) {
+    const double f = (x - dmin) / dx;
+    int a = (f == f) ? static_cast<int>(f) : 0;
+    return max(0, min(a, nx - 1));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) ngp_phi_kernel(int64_t n, const void* __restrict__ posm,
+                                                      const V4<float>* __restrict__ lo,
+                                                      GridDev g, const R* __restrict__ phi,
+                                                      R* __restrict__ pot) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x, y, z, m;
+    load_pos<R>(posm, lo, i, x, y, z, m);
+    const int64_t nx = g.nx;
+    const int64_t c = ngp_axis(x, g.domain_min, g.dx, g.nx) +
+                      ngp_axis(y, g.domain_min, g.dx, g.nx) * nx +
+                      ngp_axis(z, g.domain_min, g.dx, g.nx) * nx * nx;
+    pot[i] = phi[c];
+}
+
+// ----------------------------------------------------------------------------------------------
+// Fused particle pass of the wave strategy (one launch per step):
+//   [INTERP_CORRECT]  a = trilinear(x); v = (u + dt a) / 2                  (correct_step_)
+//   [PREDICT_DEPOSIT] v* = v + dt a; u = v + v*; x += dt/2 u; CIC(x)        (predict_step_ +
+//                                                                             deposit)
+// ----------------------------------------------------------------------------------------------
+template <typename R, bool MIXED, int MODE>
+__global__ void __launch_bounds__(256) pm_particle_kernel(PmParticleArgs a, double scale) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool active = i < a.n;
+    V4<R>* posm = static_cast<V4<R>*>(a.posm);
+    V4<float>* lo = static_cast<V4<float>*>(a.poslo);
+    V4<R>* vel = static_cast<V4<R>*>(a.vel);
+    V4<R>* accp = static_cast<V4<R>*>(a.acc);
+    V4<R>* u = static_cast<V4<R>*>(a.u);
+    const R dt = static_cast<R>(a.dt);
+    double x = 0, y = 0, z = 0, m = 0;
+    if (active) load_pos<R>(a.posm, MIXED ? lo : nullptr, i, x, y, z, m);
+
+    R vx = 0, vy = 0, vz = 0, ax = 0, ay = 0, az = 0;
+    if (active) {
+        if constexpr ((MODE & PM_INTERP_CORRECT) != 0) {
+            trilinear<R>(static_cast<const V4<R>*>(a.acc4), a.g, x, y, z, ax, ay, az);
+            const V4<R> uu = u[i];
+            vx = R(0.5) * (uu.x + dt * ax);
+            vy = R(0.5) * (uu.y + dt * ay);
+            vz = R(0.5) * (uu.z + dt * az);
+            if constexpr ((MODE & PM_WRITE_SYNC) != 0) {
+                vel[i] = v4<R>(vx, vy, vz, R(0));
+                accp[i] = v4<R>(ax, ay, az, R(0));
+            }
+        } else {
+            const V4<R> v = vel[i];
+            const V4<R> ac = accp[i];
+            vx = v.x; vy = v.y; vz = v.z;
+            ax = ac.x; ay = ac.y; az = ac.z;
+        }
+    }
+    if constexpr ((MODE & PM_PREDICT_DEPOSIT) != 0) {
+        if (active) {
+            const R sx = vx + dt * ax, sy = vy + dt * ay, sz = vz + dt * az;
+            const R ux = vx + sx, uy = vy + sy, uz = vz + sz;
+            u[i] = v4<R>(ux, uy, uz, R(0));
+            const R hdt = dt * R(0.5);
+            V4<R> p = posm[i];
+            if constexpr (MIXED) {
+                V4<float> l = lo[i];
+                df_add(p.x, l.x, hdt * ux);
+                df_add(p.y, l.y, hdt * uy);
+                df_add(p.z, l.z, hdt * uz);
+                lo[i] = l;
+                x = static_cast<double>(p.x) + l.x;
+                y = static_cast<double>(p.y) + l.y;
+                z = static_cast<double>(p.z) + l.z;
+            } else {
+                p.x = p.x + hdt * ux;
+                p.y = p.y + hdt * uy;
+                p.z = p.z + hdt * uz;
+                x = p.x;
+                y = p.y;
+                z = p.z;
+            }
+            posm[i] = p;
+        }
+        cic_deposit_warp(active, x, y, z, m, a.g, scale, a.mgrid);
+    }
+}
+
+template <typename R, bool MIXED>
+void dispatch_pm(const PmParticleArgs& a, int mode, double scale, cudaStream_t s) {
+    const int b = div_up(a.n, 256);
+    switch (mode) {
+        case PM_INTERP_CORRECT | PM_WRITE_SYNC:
+            pm_particle_kernel<R, MIXED, PM_INTERP_CORRECT | PM_WRITE_SYNC><<<b, 256, 0, s>>>(a, scale);
+            break;
+        case PM_PREDICT_DEPOSIT:
+            pm_particle_kernel<R, MIXED, PM_PREDICT_DEPOSIT><<<b, 256, 0, s>>>(a, scale);
+            break;
+        case PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT:
+            pm_particle_kernel<R, MIXED, PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT><<<b, 256, 0, s>>>(a, scale);
+            break;
+        case PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT | PM_WRITE_SYNC:
+            pm_particle_kernel<R, MIXED, PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT | PM_WRITE_SYNC>
+                <<<b, 256, 0, s>>>(a, scale);
+            break;
+        default:
+            throw Error(RRG_ERR_INVALID, "pm particle pass: unsupported mode");
+    }
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------------------------
+void launch_cic_deposit(int prec, int64_t n, const void* posm, const void* poslo,
+                        const GridDev& g, int shift_s, unsigned long long* grid,
+                        cudaStream_t s) {
+    const double scale = ldexp(1.0, shift_s);
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        cic_kernel<double><<<b, 256, 0, s>>>(n, posm, nullptr, g, scale, grid);
+    else
+        cic_kernel<float><<<b, 256, 0, s>>>(
+            n, posm, prec == RRG_PREC_MIXED ? static_cast<const V4<float>*>(poslo) : nullptr, g,
+            scale, grid);
+    RRG_LAUNCHED();
+}
+
+void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int shift_s,
+                        double dx, double rho_mean, double scale, void* src, bool zero_grid,
+                        cudaStream_t s) {
+    const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
+    const double inv_scale = ldexp(1.0, -shift_s);
+    auto* mg = const_cast<unsigned long long*>(mgrid);
+    if (prec == RRG_PREC_FP64)
+        wave_source_kernel<double><<<div_up(nc, 256), 256, 0, s>>>(
+            nc, mg, inv_scale, dx, rho_mean, scale, static_cast<double*>(src), zero_grid);
+    else
+        wave_source_kernel<float><<<div_up(nc, 256), 256, 0, s>>>(
+            nc, mg, inv_scale, dx, rho_mean, scale, static_cast<float*>(src), zero_grid);
+    RRG_LAUNCHED();
+}
+
+void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, const void* src,
+                      const WaveCoef& c, unsigned long long* maxbits, cudaStream_t s) {
+    WaveDev w;
+    w.nx = nx;
+    w.bc = c.bc_type;
+    w.uniform = (c.bc_type == RRG_BC_PERIODIC && !c.keep_layer) ? 1 : 0;
+    w.K_MAIN = c.K_MAIN;
+    w.K_ACTUAL = c.K_ACTUAL;
+    w.K_OLD = c.K_OLD;
+    w.K_F = c.K_F;
+    w.C = c.C;
+    w.DT = c.DT;
+    w.DX = c.DX;
+    w.diss_base = c.diss_base;
+    w.diss_extra = c.diss_extra;
+    w.sim_l = c.sim_l;
+    w.domain_min = c.domain_min;
+    w.bc_mass = c.bc_mass;
+    w.comx = c.com[0];
+    w.comy = c.com[1];
+    w.comz = c.com[2];
+    w.r_min = c.r_min;
+    const int gx = div_up(nx, kTX), gy = div_up(nx, kTY);
+    // z-chunk: enough blocks for ~4 resident per SM on 148 SMs
+    int zc = 32;
+    while (zc > 2 && static_cast<int64_t>(gx) * gy * div_up(nx, zc) < 592) zc >>= 1;
+    w.zc = zc;
+    dim3 grid(gx, gy, div_up(nx, zc));
+    dim3 block(kTX, kTY);
+    const bool check = maxbits != nullptr;
+#define RRG_WAVE_LAUNCH(R)                                                                    \
+    do {                                                                                      \
+        const R* p = static_cast<const R*>(phi);                                              \
+        R* po = static_cast<R*>(phi_old_inout);                                               \
+        const R* sr = static_cast<const R*>(src);                                             \
+        if (w.uniform) {                                                                      \
+            if (check) wave_step_kernel<R, true, true><<<grid, block, 0, s>>>(p, po, sr, w, maxbits); \
+            else wave_step_kernel<R, true, false><<<grid, block, 0, s>>>(p, po, sr, w, maxbits);     \
+        } else {                                                                              \
+            if (check) wave_step_kernel<R, false, true><<<grid, block, 0, s>>>(p, po, sr, w, maxbits); \
+            else wave_step_kernel<R, false, false><<<grid, block, 0, s>>>(p, po, sr, w, maxbits);     \
+        }                                                                                     \
+    } while (0)
+    if (prec == RRG_PREC_FP64) RRG_WAVE_LAUNCH(double);
+    else RRG_WAVE_LAUNCH(float);
+#undef RRG_WAVE_LAUNCH
+    RRG_LAUNCHED();
+}
+
+void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, cudaStream_t s) {
+    dim3 grid(div_up(nx, kTX), div_up(nx, kTY), nx);
+    dim3 block(kTX, kTY);
+    const double coef = -1.0 / dx;
+    if (prec == RRG_PREC_FP64)
+        gradient_kernel<double><<<grid, block, 0, s>>>(nx, coef, static_cast<const double*>(phi),
+                                                       static_cast<V4<double>*>(acc4));
+    else
+        gradient_kernel<float><<<grid, block, 0, s>>>(nx, static_cast<float>(coef),
+                                                      static_cast<const float*>(phi),
+                                                      static_cast<V4<float>*>(acc4));
+    RRG_LAUNCHED();
+}
+
+void launch_interp(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
+                   const void* acc4, void* acc, cudaStream_t s) {
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        interp_kernel<double><<<b, 256, 0, s>>>(n, posm, nullptr, g,
+                                                static_cast<const V4<double>*>(acc4),
+                                                static_cast<V4<double>*>(acc));
+    else
+        interp_kernel<float><<<b, 256, 0, s>>>(
+            n, posm, prec == RRG_PREC_MIXED ? static_cast<const V4<float>*>(poslo) : nullptr, g,
+            static_cast<const V4<float>*>(acc4), static_cast<V4<float>*>(acc));
+    RRG_LAUNCHED();
+}
+
+void launch_ngp_phi(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
+                    const void* phi, void* pot, cudaStream_t s) {
+    const int b = div_up(n, 256);
+    if (prec == RRG_PREC_FP64)
+        ngp_phi_kernel<double><<<b, 256, 0, s>>>(n, posm, nullptr, g,
+                                                 static_cast<const double*>(phi),
+                                                 static_cast<double*>(pot));
+    else
+        ngp_phi_kernel<float><<<b, 256, 0, s>>>(
+            n, posm, prec == RRG_PREC_MIXED ? static_cast<const V4<float>*>(poslo) : nullptr, g,
+            static_cast<const float*>(phi), static_cast<float*>(pot));
+    RRG_LAUNCHED();
+}
+
+void launch_pm_particles(const PmParticleArgs& a, int mode, cudaStream_t s) {
+    const double scale = ldexp(1.0, a.shift_s);
+    if (a.prec == RRG_PREC_FP64) dispatch_pm<double, false>(a, mode, scale, s);
+    else if (a.prec == RRG_PREC_MIXED) dispatch_pm<float, true>(a, mode, scale, s);
+    else dispatch_pm<float, false>(a, mode, scale, s);
+    RRG_LAUNCHED();
+}
+
+}  // namespace rrg

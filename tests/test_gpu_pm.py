@@ -1,0 +1,216 @@
+"""Particle-mesh path on the GPU against the FP64 oracle.
+
+CIC: the int64 fixed-point grid is bit-exact to the oracle's fixed-point deposit of the same
+(FP32-held) particles, and equals the reference's FP64 deposit to within the fixed-point step.
+Wave, gradient, interpolation and NGP lookups follow the reference within FP32 rounding.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import rrgsim_b200 as rg
+from helpers import disk, f32, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _grid(nx, half_width=8.0, bc_frac=0.2):
+    return rg.GridInfo.from_values(nx, 2 * half_width / nx, bc_frac)
+
+
+def _orc_grid(g: rg.GridInfo, **kw):
+    bc_frac = 1.0 - g.sim_l / g.domain_l
+    return orc.make_grid(g.nx, g.dx, bc_frac=bc_frac, **kw)
+
+
+def _ctx(prec, pos, vel, m, s2, grid):
+    c = rg.Context(0, prec)
+    c.load_particles(pos, vel, m, s2)
+    c.init_grid(grid)
+    return c
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("n,nx", [(1, 8), (300, 8), (20000, 32), (200000, 64)])
+def test_cic_fixed_point_bit_exact(prec, n, nx):
+    pos, vel, m, s2 = disk(n, seed=n)
+    # particles outside the domain and on its faces exercise the reference's clamp
+    if n >= 300:
+        pos[:5] = [[9.0, 0, 0], [-9.0, -9.0, 9.0], [8.0, 8.0, -8.0], [0.0625, 0.0625, 0.0625],
+                   [-8.0, 0.0, 7.999]]
+    g = _grid(nx)
+    with _ctx(prec, pos, vel, m, s2, g) as c:
+        c.convert_particles_to_grid()
+        mass = c.get_grid()["mass"]
+        shift = c.deposit_scale()
+    held_pos = pos if prec != "fp32" else f32(pos)
+    held_m = m if prec == "fp64" else f32(m)
+    og = _orc_grid(g)
+    q = orc.cic_fixed(held_pos, held_m, og, shift)
+    np.testing.assert_array_equal(mass, q.astype(np.float64) * 2.0 ** -shift)
+    # against the reference's FP64 deposit: within 8 half-steps of 2^-S per particle
+    ref = orc.cic_fp64(held_pos, held_m, og)
+    assert np.max(np.abs(mass - ref)) <= 8 * n * 2.0 ** -shift
+    assert abs(mass.sum() - held_m.sum()) <= 8 * n * 2.0 ** -shift
+
+
+def test_cic_run_to_run_deterministic():
+    pos, vel, m, s2 = disk(100000, seed=9)
+    g = _grid(64)
+    grids = []
+    for _ in range(2):
+        with _ctx("fp32", pos, vel, m, s2, g) as c:
+            c.convert_particles_to_grid()
+            grids.append(c.get_grid()["mass"])
+    np.testing.assert_array_equal(grids[0], grids[1])
+
+
+def _wave_setup(nx, prec, seed=11):
+    rng = np.random.default_rng(seed)
+    pos, vel, m, s2 = disk(20000, seed=seed)
+    g = _grid(nx)
+    vmax = np.max(np.linalg.norm(vel, axis=1))
+    c_speed = 10 * vmax
+    wp = rg.WaveParams.make(g.dx, diss_base=1.0 / (4 * g.dx), wave_speed=c_speed,
+                            iterations=20, setup_iterations=400, steady_check_step=30)
+    phi0 = -1.0 + 0.1 * rng.standard_normal(nx ** 3)
+    return pos, vel, m, s2, g, wp, phi0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("nx", [8, 33, 64])
+def test_wave_iteration_matches_oracle(prec, nx):
+    pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, prec)
+    with _ctx(prec, pos, vel, m, s2, g) as c:
+        c.set_wave_params(wp)
+        c.convert_particles_to_grid()
+        c.set_boundary_periodic(1.0)
+        c.set_grid_potential(phi0)
+        it, _ = c.solve_wave_equation(3)
+        got = c.get_grid()
+    assert it == 3
+    og = _orc_grid(g, wave_speed=wp.wave_speed, diss_base=wp.diss_base, bc_type=1,
+                   rho_mean=1.0 / (nx * g.dx) ** 3)
+    phi = phi0 if prec == "fp64" else f32(phi0)
+    st = orc.WaveState(nx)
+    st.set_all(phi)
+    st.solve(og, got["mass"], 3)
+    ref = st.curr
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    assert np.max(np.abs(got["grav"] - ref)) <= tol * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("bc", ["zero", "monopole", "radiative", "periodic_layer"])
+def test_wave_boundaries_match_oracle(bc):
+    nx = 24
+    pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, "fp64")
+    wp.diss_extra = 0.3
+    com = np.array([0.1, -0.05, 0.02])
+    with _ctx("fp64", pos, vel, m, s2, g) as c:
+        c.set_wave_params(wp)
+        c.convert_particles_to_grid()
+        if bc == "zero":
+            c.set_boundary_zero()
+            kw = dict(bc_type=0)
+        elif bc == "periodic_layer":
+            c.set_boundary_periodic(1.0, keep_layer=True)
+            kw = dict(bc_type=1, rho_mean=1.0 / (nx * g.dx) ** 3, keep_layer=1)
+        else:
+            c.set_boundary_monopole(1.0, com, radiative=(bc == "radiative"))
+            kw = dict(bc_type=3 if bc == "radiative" else 2, bc_mass=1.0, com=tuple(com))
+        c.set_grid_potential(phi0)
+        c.solve_wave_equation(4)
+        got = c.get_grid()
+    og = _orc_grid(g, wave_speed=wp.wave_speed, diss_base=wp.diss_base,
+                   diss_extra=wp.diss_extra, **kw)
+    st = orc.WaveState(nx)
+    st.set_all(phi0)
+    st.solve(og, got["mass"], 4)
+    np.testing.assert_allclose(got["grav"], st.curr, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_steady_state_relaxation(prec):
+    nx = 32
+    pos, vel, m, s2, g, wp, _ = _wave_setup(nx, prec)
+    wp.tolerance = 1e-4
+    wp.steady_check_step = 10
+    with _ctx(prec, pos, vel, m, s2, g) as c:
+        c.set_wave_params(wp)
+        c.convert_particles_to_grid()
+        c.set_boundary_periodic(1.0)
+        it, rel = c.solve_wave_equation(3000)
+        got = c.get_grid()
+    og = _orc_grid(g, wave_speed=wp.wave_speed, diss_base=wp.diss_base, bc_type=1,
+                   rho_mean=1.0 / (nx * g.dx) ** 3, tolerance=1e-4, steady_check_step=10)
+    st = orc.WaveState(nx)
+    rit, rrel = st.solve(og, got["mass"], 3000)
+    if prec == "fp64":
+        assert it == rit
+        assert abs(rel - rrel) <= 1e-9 * rrel
+    else:
+        assert abs(it - rit) <= 20
+    ref = st.curr
+    assert np.max(np.abs(got["grav"] - ref)) <= (1e-12 if prec == "fp64" else 1e-3) * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_gradient_and_interpolation(prec):
+    nx = 40
+    rng = np.random.default_rng(5)
+    pos, vel, m, s2 = disk(30000, seed=5)
+    pos[:4] = [[9.5, 0, 0], [-8.0, -8.0, -8.0], [7.99, 7.99, 7.99], [0.1, -0.1, 0.2]]
+    g = _grid(nx)
+    phi = np.sin(np.arange(nx ** 3) * 0.37) + 0.1 * rng.standard_normal(nx ** 3)
+    with _ctx(prec, pos, vel, m, s2, g) as c:
+        c.set_grid_potential(phi)
+        c.calc_acceleration_field()
+        c.project_grid_acceleration_on_particles()
+        c.project_grid_grav_on_particles()
+        grid = c.get_grid()
+        part = c.get_particles()
+    og = _orc_grid(g)
+    held_phi = phi if prec == "fp64" else f32(phi)
+    held_pos = f32(pos) if prec == "fp32" else pos
+    acc3 = orc.gradient(og, held_phi)
+    tol = 1e-12 if prec == "fp64" else 1e-5
+    assert np.max(np.abs(grid["acc"] - acc3)) <= tol * np.max(np.abs(acc3))
+    ref = orc.interp(held_pos, og, acc3)
+    assert np.max(np.abs(part["acc"] - ref)) <= tol * np.max(np.abs(acc3))
+    np.testing.assert_array_equal(part["grav"], orc.ngp_phi(held_pos, og, grid["grav"]))
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_pm_steps_match_oracle(prec):
+    """Disk N=20000 on a 32^3 periodic wave grid: precalc + 10 fused steps of 20 substeps."""
+    nx, n, dt, steps = 32, 20000, 2e-3, 10
+    pos, vel, m, s2 = disk(n, seed=1)
+    g = _grid(nx)
+    vmax = np.max(np.linalg.norm(vel, axis=1))
+    wp = rg.WaveParams.make(g.dx, diss_base=1.0 / (4 * g.dx), wave_speed=10 * vmax,
+                            iterations=20, setup_iterations=600, steady_check_step=1000)
+    sim = rg.SimParams(time_max=1.0, dt_save=0.1, dt_dynamics=dt, saves_without_dump=2 ** 63,
+                       use_wave_model=1)
+    with _ctx(prec, pos, vel, m, s2, g) as c:
+        c.set_wave_params(wp)
+        c.solver_init(sim)
+        c.precalc()
+        c.sync_particles_and_grid()
+        a0 = c.get_particles()["acc"]
+        c.calc_steps(steps)
+        got = c.get_particles()
+    og = _orc_grid(g, wave_speed=wp.wave_speed, diss_base=wp.diss_base, bc_type=1,
+                   rho_mean=1.0 / (nx * g.dx) ** 3, steady_check_step=1000)
+    st = orc.WaveState(nx)
+    mgrid = orc.cic_fp64(pos, m, og)
+    st.solve(og, mgrid, 600)
+    ra0 = orc.interp(pos, og, orc.gradient(og, st.curr))
+    # the deposit is int64 fixed point in every precision (2^-27 relative per contribution),
+    # so even the FP64 path differs from the reference's FP64 atomics at the 1e-8 level
+    tol_a = 1e-6 if prec == "fp64" else 1e-4
+    assert np.median(rel_err(a0, ra0)) <= tol_a
+    rp, rv, ra = orc.pm_steps(pos, vel, ra0, m, og, 20, dt, st, steps)
+    assert np.median(rel_err(got["pos"], rp)) <= (1e-10 if prec == "fp64" else 1e-5)
+    assert np.max(np.abs(got["pos"] - rp)) <= (1e-9 if prec == "fp64" else 2e-5)
+    assert np.median(rel_err(got["vel"], rv)) <= (1e-6 if prec == "fp64" else 1e-4)
+    assert np.median(rel_err(got["acc"], ra)) <= tol_a

@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the particle-mesh step (the headline workload) on B200.
+
+Workload "pm_disk_1M_128": N = 1,048,576 exponential-disk particles (G = 1, M = 1, Rd = 1,
+sech^2 z0 = 0.1, circular speed from the enclosed mass + 10% Gaussian dispersion, seed 1) on a
+128^3 periodic wave grid spanning +-8 Rd; CIC deposit, damped wave potential with c = 10 vmax,
+gamma = 1 / (4 dx / c), 20 substeps per step, trilinear interpolation, leapfrog dt = 2e-3; FP32.
+A step = predict + deposit + 20 wave substeps + gradient + interpolation + correct.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line. Under torchrun (N > 1) every rank runs an independent replica of the
+workload (the path has no data-path collective at this size): value = all ranks' particle
+steps / max-over-ranks time. `--impl reference` times the CPU restatement of the reference
+kernels (FP64, OpenMP on the host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_PART = 1 << 20
+NX = 128
+HALF = 8.0
+DT = 2e-3
+SUBSTEPS = 20
+SEED = 1
+METRIC = "PM particle-steps/s"
+UNIT = "particle-steps/s"
+WORKLOAD = "pm_disk_1M_128"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured", d
+    return 6650.0, "fallback", {}
+
+
+def make_inputs(setup_iterations: int = 20000):
+    import rrgsim_b200 as rg
+    pos, vel = rg.generate_exp_disk(SEED, N_PART, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1, 0.0, 0.0)
+    mass = np.full(N_PART, 1.0 / N_PART)
+    soft2 = np.full(N_PART, 1e-4)
+    grid = rg.GridInfo.from_values(NX, 2 * HALF / NX, 0.0)
+    vmax = float(np.max(np.linalg.norm(vel, axis=1)))
+    c = 10.0 * vmax
+    wave = rg.WaveParams.make(grid.dx, diss_base=1.0 / (4 * grid.dx), wave_speed=c,
+                              iterations=SUBSTEPS, setup_iterations=setup_iterations,
+                              tolerance=1e-6,
+                              steady_check_step=30, steady_hold_steps=3)
+    sim = rg.SimParams(time_max=1e9, dt_save=1e9, dt_dynamics=DT, saves_without_dump=0,
+                       use_wave_model=1)
+    return pos, vel, mass, soft2, grid, wave, sim
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(gpus: int):
+    if gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, 0
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist.get_rank(), dist.get_world_size(), local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------------
+def cpu_pm_sample(state, steps: int, threads: int) -> tuple[float, str]:
+    """Times `steps` PM steps of the CPU restatement (FP64, OpenMP) at full size from the given
+    relaxed state; returns (particle-steps/s, sample description)."""
+    import oracle as orc
+    pos, vel, acc, mass, phi_prev, phi_curr, grid, wave = state
+    orc.set_threads(threads)
+    og = orc.make_grid(grid.nx, grid.dx, bc_frac=0.0, wave_speed=wave.wave_speed,
+                       diss_base=wave.diss_base, bc_type=1,
+                       rho_mean=1.0 / (grid.nx * grid.dx) ** 3, steady_check_step=10 ** 9)
+    st = orc.WaveState(grid.nx)
+    st.bufs[0][:] = phi_prev
+    st.bufs[1][:] = phi_curr
+    t0 = time.perf_counter()
+    orc.pm_steps(pos, vel, acc, mass, og, SUBSTEPS, DT, st, steps)
+    el = time.perf_counter() - t0
+    return N_PART * steps / el, f"{steps} PM steps of the full workload (N=2^20, 128^3, 20 substeps)"
+
+
+def run_reference(args):
+    rank, world, _ = dist_setup(args.gpus)
+    if rank != 0:
+        barrier(world)
+        return
+    import oracle as orc
+    import rrgsim_b200 as rg
+    pos, vel, mass, soft2, grid, wave, _ = make_inputs()
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    og = orc.make_grid(grid.nx, grid.dx, bc_frac=0.0, wave_speed=wave.wave_speed,
+                       diss_base=wave.diss_base, bc_type=1,
+                       rho_mean=1.0 / (grid.nx * grid.dx) ** 3, tolerance=wave.tolerance,
+                       steady_check_step=wave.steady_check_step,
+                       steady_hold_steps=wave.steady_hold_steps)
+    # precalc as the reference: deposit, relax, gradient, interpolate (not timed). The
+    # relaxation is cut to 60 substeps here: a step costs the same whatever the potential holds.
+    st = orc.WaveState(grid.nx)
+    mg = orc.cic_fp64(pos, mass, og)
+    st.solve(og, mg, 60)
+    acc = orc.interp(pos, og, orc.gradient(og, st.curr))
+    for _ in range(min(args.warmup, 1)):
+        pos, vel, acc = orc.pm_steps(pos, vel, acc, mass, og, SUBSTEPS, DT, st, 1)
+    # each step is one full PM step; the run stops after ~90 s of steps
+    t0 = time.perf_counter()
+    done = 0
+    while done < args.steps and (done == 0 or time.perf_counter() - t0 < 90.0):
+        pos, vel, acc = orc.pm_steps(pos, vel, acc, mass, og, SUBSTEPS, DT, st, 1)
+        done += 1
+    el = time.perf_counter() - t0
+    v = N_PART * done / el
+    args.steps = done
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "particles": N_PART, "grid": NX,
+                                        "substeps": SUBSTEPS, "dt": DT},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full PM steps, FP64 OpenMP restatement of "
+                                   f"the reference kernels"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+# ------------------------------------------------------------------------------------------------
+def run_native(args):
+    import torch
+
+    import rrgsim_b200 as rg
+    rank, world, local = dist_setup(args.gpus)
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    pos, vel, mass, soft2, grid, wave, sim = make_inputs(args.setup_iterations)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = rg.Context(dev, "fp32")
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load_particles(pos, vel, mass, soft2)
+    ctx.init_grid(grid)
+    ctx.set_wave_params(wave)
+    ctx.solver_init(sim)
+    t0 = time.perf_counter()
+    ctx.precalc()
+    ctx.sync_particles_and_grid()
+    setup_s = time.perf_counter() - t0
+
+    # warm-up (records and instantiates the step graphs)
+    ctx.calc_steps(args.warmup)
+    ctx.synchronize()
+
+    # ---- device-timed region: K steps, inputs resident in HBM --------------------------------
+    clocks = ClockSampler(dev)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    l0 = rg.kernel_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ctx.calc_steps(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = rg.kernel_launch_count() - l0
+    clk = clocks.stop()
+    barrier(world)
+    el = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
+    value = N_PART * args.steps * world / el
+
+    # ---- dominant kernel: one wave substep, timed alone on the same stream --------------------
+    reps = 400
+    ctx.synchronize()
+    probe = rg.WaveParams.make(grid.dx, diss_base=wave.diss_base, wave_speed=wave.wave_speed,
+                               iterations=SUBSTEPS, steady_check_step=10 ** 9)
+    ctx.set_wave_params(probe)  # no host-synchronised steady check inside the timed launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.solve_wave_equation(8)
+    e0.record(stream)
+    ctx.solve_wave_equation(reps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wave_ms = e0.elapsed_time(e1) / reps
+    cells = NX ** 3
+    alg_bytes = 16 * cells  # read phi, phi_old, src; write phi_new (FP32)
+    hbm, how, pk = peaks()
+    achieved = alg_bytes / (wave_ms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "roofline_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("wave_step_kernel_bytes_per_launch")
+
+    # ---- end to end through the public API with host buffers ----------------------------------
+    k_e2e = min(args.steps, 50)
+    ctx2 = rg.Context(dev, "fp32")
+    ctx2.set_stream(stream.cuda_stream)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+           for k, v in dict(pos=pos, vel=vel, mass=mass, soft2=soft2).items()}
+    ctx2.init_grid(grid)
+    ctx2.set_wave_params(wave)
+    ctx2.load_particles(pin["pos"], pin["vel"], pin["mass"], pin["soft2"])
+    ctx2.solver_init(sim)
+    ctx2.precalc()
+    ctx2.sync_particles_and_grid()
+    ctx2.calc_steps(2)  # graphs recorded outside the timed region
+    ctx2.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    ctx2.load_particles(pin["pos"], pin["vel"], pin["mass"], pin["soft2"])  # H2D of the ICs
+    ctx2.sync_particles_and_grid()
+    energies = []
+    for _ in range(k_e2e):
+        ctx2.calc_steps(1)
+        energies.append(ctx2.calc_conservation()["Ek"])  # D2H of the step's diagnostics
+    snap = ctx2.get_particles()  # D2H of the final snapshot
+    e2e_el = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = N_PART * k_e2e * world / e2e_el
+    h2d = N_PART * 8 * 8 / k_e2e
+    d2h = 12 * 8 + N_PART * 10 * 8 / k_e2e
+    ctx2.close()
+    assert np.isfinite(snap["pos"]).all() and all(np.isfinite(energies))
+
+    # ---- secondary: direct-sum throughput at N = 65,536 (Plummer, FP32) ----------------------
+    direct = None
+    if rank == 0:
+        nd = 65536
+        p, v = rg.generate_plummer(0, nd, 1.0, 1.0, 20.0)
+        cd = rg.Context(dev, "fp32")
+        cd.set_stream(stream.cuda_stream)
+        cd.load_particles(p, v, np.full(nd, 1.0 / nd), np.full(nd, 1e-4))
+        cd.nbody_acceleration()
+        cd.synchronize()
+        r = 10
+        e0.record(stream)
+        for _ in range(r):
+            cd.nbody_acceleration()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / r
+        gp = nd * nd / t / 1e9
+        fp32_peak = 148 * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+        direct = {"n": nd, "gpairs_per_s": gp, "ms_per_eval": t * 1e3,
+                  "tflops_at_20_per_pair": gp * 20 / 1e3,
+                  "frac_fp32_peak": gp * 20 / 1e3 / fp32_peak,
+                  "fp32_peak_tflops": fp32_peak, "fp32_peak_kind": "nominal at sm_max_mhz"}
+        cd.close()
+
+    # ---- CPU baseline (rank 0, bounded sample) -------------------------------------------------
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        part = ctx.get_particles()
+        g = ctx.get_grid()
+        # the CPU restatement starts from the GPU's relaxed potential (both levels)
+        state = (part["pos"], part["vel"], part["acc"], mass, g["grav"], g["grav"], grid, wave)
+        threads = os.cpu_count() or 1
+        v_cpu, sample = cpu_pm_sample(state, args.cpu_steps, threads)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": sample}
+    ctx.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": N_PART, "grid": NX,
+                       "substeps": SUBSTEPS, "dt": DT, "parallelism": f"replicas{world}",
+                       "l2": "per-step working set ~140 MB > 126 MB L2; steps back to back",
+                       "setup_s": round(setup_s, 3)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": k_e2e},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "wave_step_kernel", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_kind": how,
+                         "ms_per_launch": wave_ms, "alg_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "direct_sum": direct,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--setup-iterations", type=int, default=20000,
+                    help="cap of the initial potential relaxation (profiling runs use fewer)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_native(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -117,6 +117,18 @@ def make_grid(nx: int, dx: float, bc_frac: float = 0.0, wave_speed: float = 1.0,
     return g
 
 
+def ref_lib():
+    """The reference's own CUDA build (oracle/_ref/librrgref.so, made by build_ref.sh)."""
+    dp = C.POINTER(C.c_double)
+    L = C.CDLL(str(HERE / "_ref" / "librrgref.so"))
+    L.ref_last_error.restype = C.c_char_p
+    L.ref_nbody.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp, dp, dp, dp,
+                            dp]
+    L.ref_pm.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_int, C.c_double, C.c_double, dp,
+                         C.c_double, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp]
+    return L
+
+
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
 

@@ -147,11 +147,11 @@ struct rrg_ctx {
 
 namespace {
 
-#define RRG_ENTRY(ctx, body)                                                                  \
+#define RRG_ENTRY(ctx, ...)                                                                   \
     try {                                                                                     \
         RRG_REQUIRE((ctx) != nullptr, RRG_ERR_INVALID, "null context");                       \
         RRG_CUDA(cudaSetDevice((ctx)->device));                                               \
-        body;                                                                                 \
+        __VA_ARGS__;                                                                          \
         return RRG_OK;                                                                        \
     } catch (const Error& e) {                                                                \
         if (ctx) (ctx)->err = e.what();                                                       \
@@ -532,6 +532,18 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         bool uniform = true;
         for (int64_t i = 1; i < n && uniform; ++i) uniform = (soft2[i] == soft2[0]);
 
+        // recorded graphs stay valid when the new particles reuse every buffer and launch value
+        const auto layout = [&]() {
+            return std::vector<const void*>{ctx->posm[0].p, ctx->posm[1].p, ctx->poslo[0].p,
+                                            ctx->poslo[1].p, ctx->vel.p, ctx->acc.p, ctx->u.p,
+                                            ctx->pot.p, ctx->hsoft.p, ctx->scratch.p};
+        };
+        const auto before = layout();
+        const int64_t n_before = ctx->n;
+        const int shift_before = ctx->shift_s;
+        const double hsoft_before = ctx->uniform_hsoft;
+        const bool uniform_before = ctx->soft_uniform;
+
         ctx->n = n;
         ctx->cur = 0;
         ctx->soft_uniform = uniform;
@@ -540,10 +552,6 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         ctx->sorted = false;
         ctx->time = 0.0;
         ctx->iter = 0;
-        ctx->solver_ready = false;
-        for (auto& kv : ctx->graphs)
-            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-        ctx->graphs.clear();
         {
             int e = 0;
             std::frexp(mmax > 0 ? mmax : 1.0, &e);
@@ -572,6 +580,9 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         const int rb = conservation_blocks(n);
         ctx->red_partial.alloc(static_cast<size_t>(rb) * 12 * sizeof(double));
         ctx->red_out.alloc(16 * sizeof(double));
+        if (layout() != before || n != n_before || ctx->shift_s != shift_before ||
+            ctx->uniform_hsoft != hsoft_before || ctx->soft_uniform != uniform_before)
+            drop_graphs(ctx);
 
         // stage the FP64 host arrays, then pack on the device
         const size_t stage = static_cast<size_t>(n) * 8 * sizeof(double);

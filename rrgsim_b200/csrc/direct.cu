@@ -11,6 +11,8 @@
 // FP32 and folded into the running sum once per tile (blocked summation; Kahan-compensated in
 // the MIXED precision). For small N the j-range is split over blockIdx.y and the partials are
 // reduced in FP64 in a fixed order by a second kernel (deterministic).
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace rrg {
@@ -238,6 +240,128 @@ __global__ void __launch_bounds__(kBS, 2) direct_f32_kernel(const F32Params p) {
     }
 }
 
+// ----------------------------------------------------------------------------------------------
+// Packed variant: Blackwell's paired FP32 instructions (add/mul/fma .f32x2) evaluate two pairs
+// per instruction. Each thread owns 2 G i-particles held as G float2 lanes; the j-tile is
+// staged pre-duplicated, (x, x, y, y) and (z, z, m, m), so every shared-memory broadcast
+// lands directly in the register pairs the paired instructions read. Same arithmetic per pair
+// as direct_f32_kernel (FP32 mode, tile-blocked summation).
+// ----------------------------------------------------------------------------------------------
+template <int G, bool USOFT, bool POT>
+__global__ void __launch_bounds__(kBS, 2) direct_f32x2_kernel(const F32Params p) {
+    __shared__ float4 s_xy[kBS];
+    __shared__ float4 s_zm[kBS];
+    __shared__ float2 s_h[USOFT ? 1 : kBS];
+    constexpr int IPT = 2 * G;
+    const int tid = threadIdx.x;
+    const int64_t n = p.n;
+    const int64_t ibase = static_cast<int64_t>(blockIdx.x) * (kBS * IPT);
+
+    float2 nx[G], ny[G], nz[G], hs[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        float v[2][4];
+        float h[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int64_t i = ibase + (2 * g + e) * kBS + tid;
+            V4<float> pi = v4<float>(0.f, 0.f, 0.f, 0.f);
+            h[e] = p.uniform_h;
+            if (i < n) {
+                pi = p.posm[i];
+                if constexpr (!USOFT) h[e] = p.hsoft[i];
+            }
+            v[e][0] = pi.x;
+            v[e][1] = pi.y;
+            v[e][2] = pi.z;
+        }
+        nx[g] = make_float2(-v[0][0], -v[1][0]);
+        ny[g] = make_float2(-v[0][1], -v[1][1]);
+        nz[g] = make_float2(-v[0][2], -v[1][2]);
+        hs[g] = USOFT ? make_float2(2.f * p.uniform_h, 2.f * p.uniform_h) : make_float2(h[0], h[1]);
+    }
+    float2 ax[G], ay[G], az[G], ap[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) ax[g] = ay[g] = az[g] = ap[g] = make_float2(0.f, 0.f);
+
+    const int64_t jb = static_cast<int64_t>(blockIdx.y) * p.jchunk;
+    const int64_t je = min(n, jb + p.jchunk);
+    V4<float> nxt = v4<float>(kPadPos, kPadPos, kPadPos, 0.f);
+    float nxt_h = 1.f;
+    {
+        const int64_t j = jb + tid;
+        if (j < je) {
+            nxt = p.posm[j];
+            if constexpr (!USOFT) nxt_h = p.hsoft[j];
+        }
+    }
+    for (int64_t j0 = jb; j0 < je; j0 += kBS) {
+        __syncthreads();
+        s_xy[tid] = make_float4(nxt.x, nxt.x, nxt.y, nxt.y);
+        s_zm[tid] = make_float4(nxt.z, nxt.z, nxt.w, nxt.w);
+        if constexpr (!USOFT) s_h[tid] = make_float2(nxt_h, nxt_h);
+        __syncthreads();
+        {
+            const int64_t j = j0 + kBS + tid;
+            nxt = v4<float>(kPadPos, kPadPos, kPadPos, 0.f);
+            nxt_h = 1.f;
+            if (j < je) {
+                nxt = p.posm[j];
+                if constexpr (!USOFT) nxt_h = p.hsoft[j];
+            }
+        }
+        float2 tx[G], ty[G], tz[G], tp[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) tx[g] = ty[g] = tz[g] = tp[g] = make_float2(0.f, 0.f);
+#pragma unroll 8
+        for (int k = 0; k < kBS; ++k) {
+            const float4 xy = s_xy[k];
+            const float4 zm = s_zm[k];
+            const float2 px = make_float2(xy.x, xy.y), py = make_float2(xy.z, xy.w);
+            const float2 pz = make_float2(zm.x, zm.y), pm = make_float2(zm.z, zm.w);
+            float2 hj = make_float2(0.f, 0.f);
+            if constexpr (!USOFT) hj = s_h[k];
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const float2 dx = __fadd2_rn(px, nx[g]);
+                const float2 dy = __fadd2_rn(py, ny[g]);
+                const float2 dz = __fadd2_rn(pz, nz[g]);
+                const float2 s = USOFT ? hs[g] : __fadd2_rn(hs[g], hj);
+                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, s)));
+                const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
+                const float2 minv = __fmul2_rn(pm, inv);
+                const float2 kk = __fmul2_rn(minv, __fmul2_rn(inv, inv));
+                tx[g] = __ffma2_rn(dx, kk, tx[g]);
+                ty[g] = __ffma2_rn(dy, kk, ty[g]);
+                tz[g] = __ffma2_rn(dz, kk, tz[g]);
+                if constexpr (POT) tp[g] = __fadd2_rn(tp[g], minv);
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            ax[g] = __fadd2_rn(ax[g], tx[g]);
+            ay[g] = __fadd2_rn(ay[g], ty[g]);
+            az[g] = __fadd2_rn(az[g], tz[g]);
+            if constexpr (POT) ap[g] = __fadd2_rn(ap[g], tp[g]);
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int64_t i = ibase + (2 * g + e) * kBS + tid;
+            if (i >= n) continue;
+            const float fx = e ? ax[g].y : ax[g].x, fy = e ? ay[g].y : ay[g].x,
+                        fz = e ? az[g].y : az[g].x, fp = e ? ap[g].y : ap[g].x;
+            if (gridDim.y > 1) {
+                p.part_hi[static_cast<int64_t>(blockIdx.y) * n + i] = v4<float>(fx, fy, fz, fp);
+            } else {
+                apply_epi<float, false>(p.epi, i, fx, fy, fz, -fp, POT, p.posm, p.poslo);
+            }
+        }
+    }
+}
+
 // Fixed-order FP64 reduction of the split partials, then the epilogue.
 template <bool MIXED>
 __global__ void direct_f32_finish(const F32Params p, int splits) {
@@ -350,10 +474,28 @@ void dispatch_f32(bool usoft, bool mixed, bool pot, dim3 grid, const F32Params& 
     }
 }
 
-int ipt_for(int prec, int64_t n) {
+// Kernel variants of the FP32 path: 1 = scalar, 1 i per thread; 2 = scalar, 2 i per thread;
+// 3 = paired f32x2, 2 i per thread; 4 = paired f32x2, 4 i per thread. MIXED and FP64 use the
+// scalar kernels. RRG_DIRECT_VARIANT overrides the choice (for sweeps).
+int env_variant() {
+    static const int v = [] {
+        const char* e = std::getenv("RRG_DIRECT_VARIANT");
+        return e ? std::atoi(e) : 0;
+    }();
+    return v;
+}
+
+int variant_for(int prec, int64_t n) {
     if (prec == RRG_PREC_FP64) return 1;
+    const int e = env_variant();
+    if (prec == RRG_PREC_MIXED) return (e == 1 || e == 2) ? e : (n <= 16384 ? 1 : 2);
+    if (e >= 1 && e <= 4) return e;
     return n <= 16384 ? 1 : 2;
 }
+
+int ipt_of(int variant) { return variant == 1 ? 1 : variant == 4 ? 4 : 2; }
+
+int ipt_for(int prec, int64_t n) { return ipt_of(variant_for(prec, n)); }
 
 }  // namespace
 
@@ -438,8 +580,26 @@ void launch_direct(const DirectLaunch& L) {
     RRG_REQUIRE(!mixed || L.poslo != nullptr, RRG_ERR_INVALID,
                 "direct sum: MIXED precision needs the low position parts");
     dim3 grid(static_cast<unsigned>((L.n + kBS * ipt - 1) / (kBS * ipt)), real_splits);
-    if (ipt == 1) dispatch_f32<1>(usoft, mixed, L.want_pot, grid, p, L.stream);
-    else dispatch_f32<2>(usoft, mixed, L.want_pot, grid, p, L.stream);
+    const int variant = variant_for(L.prec, L.n);
+    if (variant >= 3) {
+#define RRG_X2(G)                                                                              \
+    do {                                                                                       \
+        if (usoft) {                                                                           \
+            if (L.want_pot) direct_f32x2_kernel<G, true, true><<<grid, kBS, 0, L.stream>>>(p); \
+            else direct_f32x2_kernel<G, true, false><<<grid, kBS, 0, L.stream>>>(p);           \
+        } else {                                                                               \
+            if (L.want_pot) direct_f32x2_kernel<G, false, true><<<grid, kBS, 0, L.stream>>>(p);\
+            else direct_f32x2_kernel<G, false, false><<<grid, kBS, 0, L.stream>>>(p);          \
+        }                                                                                      \
+    } while (0)
+        if (variant == 3) RRG_X2(1);
+        else RRG_X2(2);
+#undef RRG_X2
+    } else if (ipt == 1) {
+        dispatch_f32<1>(usoft, mixed, L.want_pot, grid, p, L.stream);
+    } else {
+        dispatch_f32<2>(usoft, mixed, L.want_pot, grid, p, L.stream);
+    }
     RRG_LAUNCHED();
     if (real_splits > 1) {
         if (mixed) direct_f32_finish<true><<<div_up(L.n, 256), 256, 0, L.stream>>>(p, real_splits);

@@ -1,0 +1,140 @@
+"""Golden vectors from the reference's own CUDA build (tests/golden/make_golden.py).
+
+CPU tests pin the FP64 oracle to the reference; GPU tests hold the B200 path to the same
+fixtures. Each fixture stores its seeded inputs and the reference's outputs (FP64).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import rrgsim_b200 as rg
+from helpers import rel_err
+
+GOLD = Path(__file__).resolve().parent / "golden"
+NBODY = ["ref_nbody_plummer512", "ref_nbody_two_components512"]
+PM = ["ref_pm_disk2048_nx16", "ref_pm_disk2048_nx32_steady"]
+
+
+def load(name):
+    f = GOLD / f"{name}.npz"
+    assert f.exists(), f"missing golden fixture {f} (make it with tests/golden/make_golden.py)"
+    return dict(np.load(f))
+
+
+def pm_grid(g):
+    nx, dx, w = int(g["nx"]), float(g["dx"]), g["wave"]
+    return orc.make_grid(nx, dx, bc_frac=float(g["bc_frac"]), wave_speed=w[2], diss_base=w[0],
+                         diss_extra=w[1], bc_type=1, rho_mean=1.0 / (nx * dx) ** 3,
+                         tolerance=w[5], steady_check_step=int(w[7]),
+                         steady_hold_steps=int(w[8]))
+
+
+# ------------------------------------------------------------------------------------------------
+# oracle vs reference (CPU)
+# ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", NBODY)
+def test_oracle_nbody_matches_reference(name):
+    g = load(name)
+    acc0 = orc.direct_acc(g["pos"], g["mass"], g["soft2"])
+    assert np.max(rel_err(acc0, g["acc0"])) <= 1e-12
+    grav0 = orc.direct_grav(g["pos"], g["mass"], g["soft2"])
+    assert np.max(np.abs(grav0 - g["grav0"]) / np.abs(g["grav0"])) <= 1e-12
+    p, v, a = orc.nbody_steps(g["pos"], g["vel"], acc0, g["mass"], g["soft2"], float(g["dt"]),
+                              int(g["steps"]))
+    assert np.max(rel_err(p, g["pos_n"])) <= 1e-12
+    assert np.max(rel_err(v, g["vel_n"])) <= 1e-11
+    assert np.max(rel_err(a, g["acc_n"])) <= 1e-11
+
+
+@pytest.mark.parametrize("name", PM)
+def test_oracle_pm_matches_reference(name):
+    g = load(name)
+    og = pm_grid(g)
+    w = g["wave"]
+    mass0 = orc.cic_fp64(g["pos"], g["mass"], og)
+    np.testing.assert_allclose(mass0, g["mass0"], rtol=1e-12, atol=1e-18)
+    st = orc.WaveState(int(g["nx"]))
+    st.solve(og, mass0, int(w[3]))
+    scale = np.max(np.abs(g["phi0"]))
+    assert np.max(np.abs(st.curr - g["phi0"])) <= 1e-10 * scale
+    acc0 = orc.interp(g["pos"], og, orc.gradient(og, g["phi0"]))
+    assert np.max(rel_err(acc0, g["acc0"])) <= 1e-10
+    np.testing.assert_array_equal(orc.ngp_phi(g["pos"], og, g["phi0"]), g["grav0"])
+    p, v, a = orc.pm_steps(g["pos"], g["vel"], acc0, g["mass"], og, int(w[4]), float(g["dt"]),
+                           st, int(g["steps"]))
+    assert np.max(np.abs(p - g["pos_n"])) <= 1e-10
+    assert np.max(rel_err(v, g["vel_n"])) <= 1e-8
+    assert np.max(np.abs(st.curr - g["phi_n"])) <= 1e-9 * scale
+
+
+def test_golden_fixtures_are_nontrivial():
+    for name in NBODY + PM:
+        g = load(name)
+        assert np.isfinite(g["pos_n"]).all()
+        assert not np.allclose(g["pos_n"], g["pos"])
+    g = load(PM[0])
+    assert abs(g["mass0"].sum() - 1.0) < 1e-12  # CIC conserves the mass (all inside)
+
+
+# ------------------------------------------------------------------------------------------------
+# B200 path vs reference (GPU)
+# ------------------------------------------------------------------------------------------------
+TOL = {"fp64": 1e-9, "mixed": 1e-5, "fp32": 1e-4}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("name", NBODY)
+def test_gpu_nbody_matches_reference(name, prec):
+    g = load(name)
+    sim = rg.SimParams(time_max=1.0, dt_save=1.0, dt_dynamics=float(g["dt"]),
+                       saves_without_dump=2 ** 63, use_wave_model=0)
+    with rg.Context(0, prec) as c:
+        c.load_particles(g["pos"], g["vel"], g["mass"], g["soft2"])
+        c.solver_init(sim)
+        c.precalc()
+        s0 = c.get_particles()
+        c.calc_steps(int(g["steps"]))
+        s = c.get_particles()
+    acc_tol = {"fp64": 1e-12, "mixed": 1e-6, "fp32": 1e-5}[prec]
+    assert np.median(rel_err(s0["acc"], g["acc0"])) <= acc_tol
+    assert np.median(np.abs(s0["grav"] - g["grav0"]) / np.abs(g["grav0"])) <= acc_tol
+    assert np.max(rel_err(s["pos"], g["pos_n"])) <= (1e-4 if prec != "fp64" else 1e-12)
+    assert np.median(rel_err(s["vel"], g["vel_n"])) <= TOL[prec]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("name", PM)
+def test_gpu_pm_matches_reference(name, prec):
+    g = load(name)
+    w = g["wave"]
+    nx, dx = int(g["nx"]), float(g["dx"])
+    grid = rg.GridInfo.from_values(nx, dx, float(g["bc_frac"]))
+    wp = rg.WaveParams.make(dx, diss_base=w[0], wave_speed=w[2], diss_extra=w[1],
+                            setup_iterations=int(w[3]), iterations=int(w[4]), tolerance=w[5],
+                            print_step=int(w[6]), steady_check_step=int(w[7]),
+                            steady_hold_steps=int(w[8]))
+    sim = rg.SimParams(time_max=1.0, dt_save=1.0, dt_dynamics=float(g["dt"]),
+                       saves_without_dump=2 ** 63, use_wave_model=1)
+    with rg.Context(0, prec) as c:
+        c.load_particles(g["pos"], g["vel"], g["mass"], g["soft2"])
+        c.init_grid(grid)
+        c.set_wave_params(wp)
+        c.solver_init(sim)
+        c.precalc()
+        c.sync_particles_and_grid()
+        s0 = c.get_particles()
+        gr = c.get_grid()
+        c.calc_steps(int(g["steps"]))
+        s = c.get_particles()
+    # fixed-point deposit: within 8 contributions of 2^-S of the reference's FP64 atomics
+    assert np.max(np.abs(gr["mass"] - g["mass0"])) <= 1e-8 * np.max(g["mass0"])
+    scale = np.max(np.abs(g["phi0"]))
+    assert np.max(np.abs(gr["grav"] - g["phi0"])) <= (1e-7 if prec == "fp64" else 1e-4) * scale
+    a_tol = 1e-6 if prec == "fp64" else 1e-3
+    assert np.median(rel_err(s0["acc"], g["acc0"])) <= a_tol
+    assert np.max(np.abs(s["pos"] - g["pos_n"])) <= (1e-9 if prec == "fp64" else 1e-5)
+    assert np.median(rel_err(s["vel"], g["vel_n"])) <= (1e-6 if prec == "fp64" else 1e-4)

@@ -346,6 +346,17 @@ RRG_API rrg_status rrg_dev_direct_vjp_f32(const void* posm, const void* hsoft,
                                           float uniform_hsoft, int64_t n, const void* lam,
                                           void* out, void* stream);
 
+/* Same result as rrg_dev_direct_forces_f32 in RRG_PREC_FP32, for callers that cannot let a
+ * library allocate device memory (a host that reserves its whole memory budget up front, a
+ * plugin inside another framework's allocator, a loop that must not risk an allocation). It
+ * allocates nothing: its scratch is one fixed 4 MiB device array per GPU, held until the
+ * process exits. n must be in [1, 1048576]; larger n is RRG_ERR_INVALID. The first call on a
+ * device looks up that array's device address (make it before any stream capture). All calls
+ * share the array: calls that overlap on the GPU race. No counterpart in the reference. */
+RRG_API rrg_status rrg_dev_direct_forces_f32_noalloc(const void* posm, const void* hsoft,
+                                                     float uniform_hsoft, int64_t n, void* out,
+                                                     void* stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

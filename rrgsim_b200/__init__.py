@@ -157,6 +157,7 @@ def lib() -> C.CDLL:
                                        C.c_double, d, d]),
         "rrg_dev_direct_forces_f32": (st, [vp, vp, vp, C.c_float, i64, vp, i32, vp]),
         "rrg_dev_direct_vjp_f32": (st, [vp, vp, C.c_float, i64, vp, vp, vp]),
+        "rrg_dev_direct_forces_f32_noalloc": (st, [vp, vp, C.c_float, i64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

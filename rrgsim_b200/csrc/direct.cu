@@ -11,6 +11,7 @@
 // FP32 and folded into the running sum once per tile (blocked summation; Kahan-compensated in
 // the MIXED precision). For small N the j-range is split over blockIdx.y and the partials are
 // reduced in FP64 in a fixed order by a second kernel (deterministic).
+#include <algorithm>
 #include <cstdlib>
 
 #include "kernels.cuh"
@@ -490,31 +491,61 @@ int variant_for(int prec, int64_t n) {
     const int e = env_variant();
     if (prec == RRG_PREC_MIXED) return (e == 1 || e == 2) ? e : (n <= 16384 ? 1 : 2);
     if (e >= 1 && e <= 4) return e;
-    return n <= 16384 ? 1 : 2;
+    // measured on B200 (Plummer, FP32): the paired kernels lead from N = 16k on; 4 i-particles
+    // per thread pay off once there are enough blocks to fill the machine
+    return n < 131072 ? 3 : 4;
 }
 
 int ipt_of(int variant) { return variant == 1 ? 1 : variant == 4 ? 4 : 2; }
 
 int ipt_for(int prec, int64_t n) { return ipt_of(variant_for(prec, n)); }
 
+// Resident 256-thread blocks per SM of the kernel a variant launches (queried once).
+int resident_blocks(int prec, int variant) {
+    static int cache[3][5] = {};
+    int& r = cache[prec][variant];
+    if (r) return r;
+    const void* k = nullptr;
+    if (prec == RRG_PREC_FP64) k = reinterpret_cast<const void*>(&direct_f64_kernel<true, false>);
+    else if (prec == RRG_PREC_MIXED)
+        k = variant == 1 ? reinterpret_cast<const void*>(&direct_f32_kernel<1, true, true, false>)
+                         : reinterpret_cast<const void*>(&direct_f32_kernel<2, true, true, false>);
+    else if (variant == 1) k = reinterpret_cast<const void*>(&direct_f32_kernel<1, true, false, false>);
+    else if (variant == 2) k = reinterpret_cast<const void*>(&direct_f32_kernel<2, true, false, false>);
+    else if (variant == 3) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<1, true, false>);
+    else k = reinterpret_cast<const void*>(&direct_f32x2_kernel<2, true, false>);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kBS, 0) != cudaSuccess || nb < 1) {
+        (void)cudaGetLastError();
+        nb = 1;
+    }
+    r = nb;
+    return r;
+}
+
 }  // namespace
 
+// j-split count: the smallest one whose block count fills whole waves of resident blocks to
+// within 2% of the best achievable (wave quantisation is what costs at these sizes; each
+// extra split only adds n x 16 B of partials and a tiny reduction).
 int direct_choose_splits(int prec, int64_t n, int sms) {
-    const int ipt = ipt_for(prec, n);
+    const int variant = variant_for(prec, n);
+    const int ipt = ipt_of(variant);
     const int64_t iblocks = (n + kBS * ipt - 1) / (kBS * ipt);
     const int64_t tiles = (n + kBS - 1) / kBS;
-    const int64_t slots = static_cast<int64_t>(sms) * 2;  // two resident blocks per SM
-    if (iblocks >= slots) return 1;
-    // smallest split count that fills the machine with >= 90% wave efficiency
-    int best = 1;
-    for (int64_t sp = 1; sp <= tiles && sp <= 64; ++sp) {
+    const int64_t slots = static_cast<int64_t>(sms) * resident_blocks(prec, variant);
+    double eff[65] = {};
+    double best = 0.0;
+    const int64_t top = std::min<int64_t>(tiles, 64);
+    for (int64_t sp = 1; sp <= top; ++sp) {
         const int64_t total = iblocks * sp;
         const int64_t waves = (total + slots - 1) / slots;
-        const double eff = static_cast<double>(total) / static_cast<double>(waves * slots);
-        best = static_cast<int>(sp);
-        if (total >= slots && eff >= 0.9) break;
+        eff[sp] = static_cast<double>(total) / static_cast<double>(waves * slots);
+        best = std::max(best, eff[sp]);
     }
-    return best;
+    for (int64_t sp = 1; sp <= top; ++sp)
+        if (eff[sp] >= best - 0.02) return static_cast<int>(sp);
+    return 1;
 }
 
 size_t direct_scratch_bytes(int prec, int64_t n, int splits) {

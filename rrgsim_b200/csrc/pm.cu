@@ -215,57 +215,36 @@ template <typename R, bool UNIFORM, bool CHECK>
 __global__ void __launch_bounds__(kTX* kTY) wave_step_kernel(
     const R* __restrict__ phi, R* __restrict__ phi_old, const R* __restrict__ src,
     const WaveDev w, unsigned long long* __restrict__ maxbits) {
-    __shared__ R tile[kTY + 2][kTX + 2];
+    // One thread per (x, y) column marches through zc planes: phi(z - 1), phi(z), phi(z + 1)
+    // stay in registers, the four in-plane neighbours come through L1 (adjacent threads share
+    // their cache lines). No shared memory, no barriers. int32 indexing: nx <= 1024.
     const int nx = w.nx;
-    const int64_t nx2 = static_cast<int64_t>(nx) * nx;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * kTX + tx;
-    const int x = blockIdx.x * kTX + tx;
-    const int y = blockIdx.y * kTY + ty;
+    const int plane = nx * nx;
+    const int tid = threadIdx.y * kTX + threadIdx.x;
+    const int x = blockIdx.x * kTX + threadIdx.x;
+    const int y = blockIdx.y * kTY + threadIdx.y;
     const bool valid = (x < nx) && (y < nx);
     const bool periodic = (w.bc == RRG_BC_PERIODIC);
-    // coordinates used for loads: wrapped (periodic) or clamped (others; values then unused)
-    const int xl = periodic ? wrap_mod(x, nx) : min(x, nx - 1);
-    const int yl = periodic ? wrap_mod(y, nx) : min(y, nx - 1);
-    const int z0 = blockIdx.z * w.zc;
-    const int z1 = min(nx, z0 + w.zc);
-
-    // halo cell handled by this thread (80 halo cells: two rows of 32, two columns of 8)
-    int hsx = -1, hsy = -1, hgx = 0, hgy = 0;
-    if (tid < 2 * kTX + 2 * kTY) {
-        if (tid < kTX) { hsx = tid + 1; hsy = 0; }
-        else if (tid < 2 * kTX) { hsx = tid - kTX + 1; hsy = kTY + 1; }
-        else if (tid < 2 * kTX + kTY) { hsx = 0; hsy = tid - 2 * kTX + 1; }
-        else { hsx = kTX + 1; hsy = tid - 2 * kTX - kTY + 1; }
-        const int gx = blockIdx.x * kTX + hsx - 1;
-        const int gy = blockIdx.y * kTY + hsy - 1;
-        hgx = periodic ? wrap_mod(gx, nx) : max(0, min(gx, nx - 1));
-        hgy = periodic ? wrap_mod(gy, nx) : max(0, min(gy, nx - 1));
-    }
-
-    auto zidx = [&](int z) -> int64_t {
-        const int zz = periodic ? wrap_mod(z, nx) : max(0, min(z, nx - 1));
-        return zz * nx2;
-    };
-    const int64_t col = xl + static_cast<int64_t>(yl) * nx;
-    R pm = phi[col + zidx(z0 - 1)];
-    R pc = phi[col + zidx(z0)];
-
     double dmax = 0.0, amax = 0.0;
-    for (int z = z0; z < z1; ++z) {
-        const R pn = phi[col + zidx(z + 1)];
-        R hval = R(0);
-        if (hsx >= 0) hval = phi[hgx + static_cast<int64_t>(hgy) * nx + zidx(z)];
-        __syncthreads();
-        tile[ty + 1][tx + 1] = pc;
-        if (hsx >= 0) tile[hsy][hsx] = hval;
-        __syncthreads();
-        if (valid) {
-            const int64_t c = x + static_cast<int64_t>(y) * nx + z * nx2;
-            const bool on_edge = x == 0 || x == nx - 1 || y == 0 || y == nx - 1 || z == 0 ||
-                                 z == nx - 1;
+    if (valid) {
+        // in-plane neighbour offsets: periodic wrap, or clamped (unused on the boundary nodes)
+        const int oxm = x > 0 ? -1 : (periodic ? nx - 1 : 0);
+        const int oxp = x < nx - 1 ? 1 : (periodic ? -(nx - 1) : 0);
+        const int oym = y > 0 ? -nx : (periodic ? (nx - 1) * nx : 0);
+        const int oyp = y < nx - 1 ? nx : (periodic ? -(nx - 1) * nx : 0);
+        const bool xy_edge = x == 0 || x == nx - 1 || y == 0 || y == nx - 1;
+        const int col = x + y * nx;
+        const int z0 = blockIdx.z * w.zc;
+        const int z1 = min(nx, z0 + w.zc);
+        const int zm0 = z0 > 0 ? z0 - 1 : (periodic ? nx - 1 : 0);
+        R pm = __ldg(phi + col + zm0 * plane);
+        R pc = __ldg(phi + col + z0 * plane);
+        for (int z = z0; z < z1; ++z) {
+            const int zn = z < nx - 1 ? z + 1 : (periodic ? 0 : nx - 1);
+            const R pn = __ldg(phi + col + zn * plane);
+            const int c = col + z * plane;
             R out;
-            if (!periodic && on_edge) {
+            if (!periodic && (xy_edge || z == 0 || z == nx - 1)) {
                 double v = 0.0;
                 if (w.bc == RRG_BC_MONOPOLE_DIRICHLET)
                     v = monopole_phi(w, w.domain_min + x * w.DX, w.domain_min + y * w.DX,
@@ -274,8 +253,8 @@ __global__ void __launch_bounds__(kTX* kTY) wave_step_kernel(
                     v = radiative_value<R>(w, phi, x, y, z);
                 out = static_cast<R>(v);
             } else {
-                const R lap = tile[ty + 1][tx] + tile[ty + 1][tx + 2] + tile[ty][tx + 1] +
-                              tile[ty + 2][tx + 1] + pm + pn;
+                const R lap = __ldg(phi + c + oxm) + __ldg(phi + c + oxp) +
+                              __ldg(phi + c + oym) + __ldg(phi + c + oyp) + pm + pn;
                 R kmain, kact, kold, kf;
                 if constexpr (UNIFORM) {
                     kmain = static_cast<R>(w.K_MAIN);
@@ -302,9 +281,9 @@ __global__ void __launch_bounds__(kTX* kTY) wave_step_kernel(
                 dmax = fmax(dmax, fabs(static_cast<double>(out) - static_cast<double>(pc)));
                 amax = fmax(amax, fabs(static_cast<double>(out)));
             }
+            pm = pc;
+            pc = pn;
         }
-        pm = pc;
-        pc = pn;
     }
     if constexpr (CHECK) {
         // warp max -> block max -> one atomicMax per block on the (non-negative) double bits
@@ -590,9 +569,26 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
     w.comz = c.com[2];
     w.r_min = c.r_min;
     const int gx = div_up(nx, kTX), gy = div_up(nx, kTY);
-    // z-chunk: enough blocks for ~4 resident per SM on 148 SMs
+    // z-chunk: trade wave efficiency (blocks against 8 resident 256-thread blocks per SM)
+    // against the one extra plane each column loads per chunk
+    int dev = 0;
+    RRG_CUDA(cudaGetDevice(&dev));
+    static int sms = 0;
+    if (!sms) sms = num_sms(dev);
+    const int64_t slots = static_cast<int64_t>(sms) * 8;
     int zc = 32;
-    while (zc > 2 && static_cast<int64_t>(gx) * gy * div_up(nx, zc) < 592) zc >>= 1;
+    double best = -1.0;
+    for (int cand : {2, 4, 8, 16, 32, 64}) {
+        if (cand > nx && cand != 2) break;
+        const int64_t blocks = static_cast<int64_t>(gx) * gy * div_up(nx, cand);
+        const int64_t waves = (blocks + slots - 1) / slots;
+        const double eff = static_cast<double>(blocks) / static_cast<double>(waves * slots) *
+                           cand / (cand + 1.0);
+        if (eff > best + 1e-9) {
+            best = eff;
+            zc = cand;
+        }
+    }
     w.zc = zc;
     dim3 grid(gx, gy, div_up(nx, zc));
     dim3 block(kTX, kTY);

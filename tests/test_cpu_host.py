@@ -165,3 +165,35 @@ def test_generators_deterministic_and_shaped():
     # median radius of an exponential disk: 1.678 Rd
     assert abs(np.median(R) - 1.678) < 0.05
     assert abs(np.median(np.abs(pd[:, 2])) - 0.1 * np.arctanh(0.5)) < 0.01
+
+
+@pytest.mark.parametrize("fault", ["no_params", "bad_json", "missing_ic", "truncated_ic",
+                                   "short_row"])
+def test_rrgsim_executable_reports_host_faults(tmp_path, fault):
+    """Failures on the host side end the run with exit code 1 and a message, before any GPU
+    work (the reference logs them and exits 0)."""
+    import subprocess
+    rng = np.random.default_rng(0)
+    pos, vel = rng.standard_normal((8, 3)), rng.standard_normal((8, 3))
+    (tmp_path / "ini").mkdir()
+    rg.write_ic_text(tmp_path / "ini" / "S.txt", pos, vel)
+    d = json.loads(json.dumps(SAMPLE))
+    d.pop("grid_params")
+    d.pop("wave_params")
+    if fault == "missing_ic":
+        d["ini_params"]["ini_file_star"] = "ini/none.txt"
+    if fault == "truncated_ic":
+        lines = (tmp_path / "ini" / "S.txt").read_text().splitlines()
+        (tmp_path / "ini" / "S.txt").write_text("\n".join(lines[:5]) + "\n")
+    if fault == "short_row":
+        lines = (tmp_path / "ini" / "S.txt").read_text().splitlines()
+        lines[3] = "1 2 3"
+        (tmp_path / "ini" / "S.txt").write_text("\n".join(lines) + "\n")
+    if fault != "no_params":
+        text = json.dumps(d)
+        (tmp_path / "params.json").write_text(text[:-3] if fault == "bad_json" else text)
+    r = subprocess.run([str(rg.BIN_PATH), str(tmp_path)], capture_output=True, text=True,
+                       env={"RRGSIM_QUIET": "1", "PATH": "/usr/bin:/bin"}, timeout=120)
+    assert r.returncode == 1
+    assert "rrgsim:" in r.stderr
+    assert not (tmp_path / "dump").exists()

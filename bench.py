@@ -281,10 +281,12 @@ def run_native(args):
     traffic = None
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("wave_step_kernel_bytes_per_launch")
+        traffic = json.loads(tf.read_text()).get("wave_periodic_kernel_bytes_per_launch")
 
     # ---- end to end through the public API with host buffers ----------------------------------
-    k_e2e = min(args.steps, 50)
+    # the same run length as the device-timed region: ICs up once, K steps each followed by a
+    # read of that step's diagnostics, the final snapshot down
+    k_e2e = args.steps
     ctx2 = rg.Context(dev, "fp32")
     ctx2.set_stream(stream.cuda_stream)
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
@@ -364,7 +366,7 @@ def run_native(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": k_e2e},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "wave_step_kernel", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "wave_periodic_kernel", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_kind": how,
                          "ms_per_launch": wave_ms, "alg_bytes_per_launch": alg_bytes},

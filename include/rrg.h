@@ -328,6 +328,94 @@ RRG_API rrg_status rrg_generate_exp_disk(uint64_t seed, int64_t n, double disk_m
                                          double bulge_a, double* pos, double* vel);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Batched ensemble of independent galaxies (no counterpart in the reference, which runs one  */
+/* simulation per process). Each galaxy follows the N-body strategy                           */
+/* (solver/app/include/rrgsim_integration_nbody.cuh:50-56) in FP32, all galaxies in one      */
+/* persistent force launch over a device work-list, steps replayed as CUDA graphs.            */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rrg_ensemble rrg_ensemble;
+
+/* counts[g] particles per galaxy; pos/vel (total x 3), mass (total) concatenated galaxy after
+ * galaxy; soft2_per_galaxy[g] is each galaxy's softening squared. autotune_tiles != 0 times
+ * the tile variants and j-chunk sizes on this work-list and keeps the fastest. Computes the
+ * initial accelerations. */
+RRG_API rrg_status rrg_ensemble_create(int device, int ngal, const int64_t* counts,
+                                       const double* pos, const double* vel,
+                                       const double* mass, const double* soft2_per_galaxy,
+                                       double dt, int autotune_tiles, rrg_ensemble** out);
+RRG_API rrg_status rrg_ensemble_destroy(rrg_ensemble* e);
+RRG_API rrg_status rrg_ensemble_set_stream(rrg_ensemble* e, void* stream);
+/* nsteps leapfrog steps of every galaxy (batched, graph-replayed). */
+RRG_API rrg_status rrg_ensemble_step(rrg_ensemble* e, int nsteps);
+/* The same steps with one unbatched force launch per galaxy (comparison baseline). plain != 0
+ * launches in the reference's shape (acceleration_kernel_blocked_, nbody.cu:19-65 and
+ * :200-213: one i-particle per thread, 256-thread blocks, no j-split); plain == 0 uses the
+ * library's single-galaxy kernel without a j-split. */
+RRG_API rrg_status rrg_ensemble_step_sequential(rrg_ensemble* e, int nsteps, int plain);
+RRG_API rrg_status rrg_ensemble_synchronize(rrg_ensemble* e);
+/* Downloads the state (any pointer may be NULL), in the order given at creation. */
+RRG_API rrg_status rrg_ensemble_get(rrg_ensemble* e, double* pos, double* vel, double* acc);
+/* The tile variant (1: 2 i-particles per thread, 2: 4), j-chunk, work items and the timed
+ * force evaluation the autotuner settled on. */
+RRG_API rrg_status rrg_ensemble_tuning(const rrg_ensemble* e, int* variant, int* jchunk,
+                                       int* num_items, double* force_ms);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Differentiable direct N-body (no counterpart in the reference). Hand-written adjoint of    */
+/* the leapfrog of nbody.cu:122-181 with the direct-sum force of nbody.cu:19-65: one         */
+/* vector-Jacobian product of the force per step, states recomputed from checkpoints.        */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rrg_adjoint rrg_adjoint;
+
+/* precision RRG_PREC_FP32 or RRG_PREC_FP64; soft2 has n entries; checkpoint_every K > 0
+ * keeps (x, v) every K steps and recomputes the steps between (K <= 0: keep only the start). */
+RRG_API rrg_status rrg_adjoint_create(int device, int precision, int64_t n, double dt,
+                                      int nsteps, int checkpoint_every, const double* soft2,
+                                      rrg_adjoint** out);
+RRG_API rrg_status rrg_adjoint_destroy(rrg_adjoint* a);
+/* Device memory in the object's precision: x0[i] = (x, y, z, m), v0[i] = (vx, vy, vz, 0), both
+ * n x 4. Runs nsteps leapfrog steps; x_out / v_out (may be NULL) receive the final state.
+ * Checks on the device whether all masses are equal (equal masses take faster kernels in
+ * FP32), which waits for the stream once per call. */
+RRG_API rrg_status rrg_adjoint_forward(rrg_adjoint* a, const void* x0, const void* v0,
+                                       void* x_out, void* v_out, void* stream);
+/* Cotangents of the final (x, v) (n x 4, w ignored; NULL = zero) in; out gx[i] = (dL/dx,
+ * dL/dy, dL/dz, dL/dm) and gv[i] = (dL/dvx, dL/dvy, dL/dvz, 0) of the initial state. */
+RRG_API rrg_status rrg_adjoint_backward(rrg_adjoint* a, const void* gx_final,
+                                        const void* gv_final, void* gx_out, void* gv_out,
+                                        void* stream);
+/* enabled = 0: backward skips dL/dm (the w slot of gx_out is then 0), which saves about a sixth
+ * of the FP32 pair work. Default 1. */
+RRG_API rrg_status rrg_adjoint_set_mass_gradient(rrg_adjoint* a, int enabled);
+/* Differentiable particle-mesh steps (periodic wave potential): hand-written adjoint of the
+ * RectWave step (solver/app/include/rrgsim_integration_rect.cuh:99-112) — trilinear-gather
+ * adjoint of the CIC deposit, CIC-scatter adjoint of the interpolation, transposed gradient,
+ * time-reversed wave stencil. The initial potential is a fixed input. */
+typedef struct rrg_pm_adjoint rrg_pm_adjoint;
+/* m_max: the largest particle mass (sets the deposit's fixed-point scale); total_mass_for_rho:
+ * the mass whose mean density the periodic source subtracts (1 in the reference's precalc);
+ * wave->iterations substeps per step with wave->dt, wave_speed and diss_base. */
+RRG_API rrg_status rrg_pm_adjoint_create(int device, int precision, int64_t n, double m_max,
+                                         const rrg_grid_info* grid, const rrg_wave_params* wave,
+                                         double total_mass_for_rho, double dt, int nsteps,
+                                         int checkpoint_every, rrg_pm_adjoint** out);
+RRG_API rrg_status rrg_pm_adjoint_destroy(rrg_pm_adjoint* a);
+/* x0 (x, y, z, m), v0: n x 4 device memory of the precision; phi_prev0 / phi_cur0: the two
+ * wave levels (nx^3) the steps start from. */
+RRG_API rrg_status rrg_pm_adjoint_forward(rrg_pm_adjoint* a, const void* x0, const void* v0,
+                                          const void* phi_prev0, const void* phi_cur0,
+                                          void* x_out, void* v_out, void* phi_out, void* stream);
+RRG_API rrg_status rrg_pm_adjoint_backward(rrg_pm_adjoint* a, const void* gx_final,
+                                           const void* gv_final, void* gx_out, void* gv_out,
+                                           void* stream);
+
+/* Vector-Jacobian product of the direct-sum acceleration in FP32 or FP64 on caller memory:
+ * posm/lam/out n x 4 of that precision (out[i] = (dx, dy, dz, dm)); hsoft NULL = uniform. */
+RRG_API rrg_status rrg_dev_direct_vjp(const void* posm, const void* hsoft, double uniform_hsoft,
+                                      int64_t n, const void* lam, void* out, int precision,
+                                      void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Raw device kernels on caller memory (used by the Python/torch binding)                     */
 /* ------------------------------------------------------------------------------------------ */
 

@@ -267,6 +267,21 @@ def ngp_phi(pos, g: Grid, phi) -> np.ndarray:
     return out
 
 
+def ngp_project(pos, g: Grid, values) -> np.ndarray:
+    """NGP cell average of per-particle values: every particle adds value / (particles in its
+    cell) to its cell (deposit_cell_grav_NGP_ / deposit_cell_acc_NGP_, rm_p2mesh.cu:142-174,
+    cell counts from assign_particles_to_cells_, rm_p2mesh.cu:25-66). values is (n,) or (n, k);
+    the result is (nx^3,) or (nx^3, k). Summation order is numpy's; the reference's is that of
+    its atomics."""
+    values = _f64(values)
+    cell = ngp_cell(pos, g)
+    count = np.bincount(cell, minlength=g.nx ** 3).astype(np.float64)
+    share = values / (count[cell] if values.ndim == 1 else count[cell][:, None])
+    out = np.zeros((g.nx ** 3,) + values.shape[1:])
+    np.add.at(out, cell, share)
+    return out
+
+
 def pm_steps(pos, vel, acc, mass, g: Grid, iterations: int, dt: float, wave: WaveState,
              nsteps: int):
     """RectWaveIntegrationSolver::calc_step, nsteps times. Returns (pos, vel, acc)."""

@@ -158,6 +158,16 @@ def lib() -> C.CDLL:
         "rrg_dev_direct_forces_f32": (st, [vp, vp, vp, C.c_float, i64, vp, i32, vp]),
         "rrg_dev_direct_vjp_f32": (st, [vp, vp, C.c_float, i64, vp, vp, vp]),
         "rrg_dev_direct_forces_f32_noalloc": (st, [vp, vp, C.c_float, i64, vp, vp]),
+        "rrg_ensemble_create": (st, [i32, i32, C.POINTER(i64), d, d, d, d, C.c_double, i32,
+                                     C.POINTER(vp)]),
+        "rrg_ensemble_destroy": (st, [vp]),
+        "rrg_ensemble_set_stream": (st, [vp, vp]),
+        "rrg_ensemble_step": (st, [vp, i32]),
+        "rrg_ensemble_step_sequential": (st, [vp, i32, i32]),
+        "rrg_ensemble_synchronize": (st, [vp]),
+        "rrg_ensemble_get": (st, [vp, d, d, d]),
+        "rrg_ensemble_tuning": (st, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), d]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -336,6 +346,97 @@ class Context:
 
     def set_sort_interval(self, interval: int) -> None:
         self._c(lib().rrg_set_sort_interval(self._h, int(interval)))
+
+
+class Ensemble:
+    """Independent galaxies stepped together (one persistent force launch per step)."""
+
+    def __init__(self, counts, pos, vel, mass, soft2_per_galaxy, dt: float, device: int = 0,
+                 autotune: bool = True):
+        counts = np.ascontiguousarray(counts, dtype=np.int64)
+        pos, vel, mass = _f64(pos), _f64(vel), _f64(mass)
+        s2 = _f64(soft2_per_galaxy)
+        self.counts = counts
+        self.ntot = int(counts.sum())
+        if pos.shape != (self.ntot, 3) or vel.shape != (self.ntot, 3) or mass.shape != (self.ntot,):
+            raise RRGError(1, "Ensemble: arrays must hold sum(counts) particles")
+        self._h = C.c_void_p()
+        check(lib().rrg_ensemble_create(int(device), len(counts),
+                                        counts.ctypes.data_as(C.POINTER(C.c_int64)), _d(pos),
+                                        _d(vel), _d(mass), _d(s2), float(dt), int(autotune),
+                                        C.byref(self._h)))
+
+    def _c(self, status):
+        check(status, None)
+
+    def step(self, nsteps: int) -> None:
+        self._c(lib().rrg_ensemble_step(self._h, int(nsteps)))
+
+    def step_sequential(self, nsteps: int, plain: bool = False) -> None:
+        """One force launch per galaxy; plain=True in the reference's launch shape."""
+        self._c(lib().rrg_ensemble_step_sequential(self._h, int(nsteps), int(plain)))
+
+    def set_stream(self, stream_ptr) -> None:
+        self._c(lib().rrg_ensemble_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def synchronize(self) -> None:
+        self._c(lib().rrg_ensemble_synchronize(self._h))
+
+    def get(self) -> dict:
+        pos, vel, acc = (np.empty((self.ntot, 3)) for _ in range(3))
+        self._c(lib().rrg_ensemble_get(self._h, _d(pos), _d(vel), _d(acc)))
+        return {"pos": pos, "vel": vel, "acc": acc}
+
+    def tuning(self) -> dict:
+        v, j, k = C.c_int(), C.c_int(), C.c_int()
+        ms = C.c_double()
+        self._c(lib().rrg_ensemble_tuning(self._h, C.byref(v), C.byref(j), C.byref(k),
+                                          C.byref(ms)))
+        return {"variant": v.value, "jchunk": j.value, "items": k.value, "force_ms": ms.value}
+
+    def close(self) -> None:
+        if self._h:
+            lib().rrg_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def make_ensemble(ngal: int = 64, nmin: int = 1024, nmax: int = 65536, seed: int = 3,
+                  base_mass: float = 1.0, base_scale: float = 1.0, base_soft: float = 0.01):
+    """The batched-form galaxies: N log-uniform in [nmin, nmax], each a Plummer sphere or an
+    exponential disk by coin flip, mass / scale radius / softening each uniform in
+    [0.5, 2] x base. Returns counts, pos, vel, mass, soft2 per galaxy."""
+    rng = np.random.default_rng(seed)
+    counts, P, V, M, S2 = [], [], [], [], []
+    for g in range(ngal):
+        n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        disk_kind = rng.random() < 0.5
+        mass, scale, soft = (base_mass * rng.uniform(0.5, 2.0), base_scale * rng.uniform(0.5, 2.0),
+                             base_soft * rng.uniform(0.5, 2.0))
+        gseed = int(rng.integers(1 << 62))
+        if disk_kind:
+            p, v = generate_exp_disk(gseed, n, mass, scale, 0.1 * scale, 7.5 * scale,
+                                     7.5 * scale, 0.1)
+        else:
+            p, v = generate_plummer(gseed, n, mass, scale, 20.0 * scale)
+        counts.append(n)
+        P.append(p)
+        V.append(v)
+        M.append(np.full(n, mass / n))
+        S2.append(soft * soft)
+    return (np.array(counts, dtype=np.int64), np.vstack(P), np.vstack(V), np.concatenate(M),
+            np.array(S2))
 
 
 # -- host I/O --------------------------------------------------------------------------------

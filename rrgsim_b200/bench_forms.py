@@ -1,6 +1,6 @@
 """Measurements of the secondary forms of the hot path (one JSON line per form).
 
-    python -m rrgsim_b200.bench_forms [plummer|precision|ensemble|adjoint|all]
+    python -m rrgsim_b200.bench_forms [plummer|precision|ensemble|adjoint|adjoint_pm|vjp|all]
 
 plummer   : Plummer N = 4096, eps = 0.01, dt = 1e-3, 100 steps, a snapshot every 10 steps.
 precision : bulge (Plummer M = 0.2, a = 0.2) + disk (M = 0.8, Rd = 1), N = 65,536 direct sum over
@@ -12,6 +12,8 @@ ensemble  : 64 galaxies, N log-uniform in [1024, 65536] (seed 3), 500 steps batc
 adjoint   : gradient of the mean squared final-position error through 200 leapfrog steps
             (N = 16,384 Plummer, eps = 0.02, dt = 1e-3, checkpoints every 20 steps) vs the
             forward pass.
+adjoint_pm: the same through the particle-mesh step (N = 262,144 disk, 64^3, 20 substeps).
+vjp       : one force vector-Jacobian product vs one force evaluation, N = 16,384 and 65,536.
 All inputs are synthetic (the reference ships no benchmark data). Times are CUDA events on
 the stream the library launches on.
 """
@@ -159,10 +161,15 @@ def form_ensemble(torch, steps=500):
     pairs = float((counts.astype(np.float64) ** 2).sum())
     s = torch.cuda.Stream()
     res = {}
-    for mode in ("batched", "sequential"):
+    for mode in ("batched", "sequential", "sequential_plain"):
         with rg.Ensemble(counts, pos, vel, mass, s2, 1e-3, autotune=(mode == "batched")) as e:
             e.set_stream(s.cuda_stream)
-            run = e.step if mode == "batched" else e.step_sequential
+            if mode == "batched":
+                run = e.step
+            elif mode == "sequential":
+                run = e.step_sequential
+            else:
+                run = lambda k: e.step_sequential(k, plain=True)  # noqa: E731
             k = steps if mode == "batched" else 20
             run(2)
             e.synchronize()
@@ -175,9 +182,12 @@ def form_ensemble(torch, steps=500):
             if mode == "batched":
                 res[mode]["tuning"] = e.tuning()
     b_ms, s_ms = res["batched"]["ms_per_step"], res["sequential"]["ms_per_step"]
+    p_ms = res["sequential_plain"]["ms_per_step"]
     return {"form": "ensemble_64", "galaxies": len(counts), "particles": int(counts.sum()),
             "pairs_per_step": pairs, "batched_ms_per_step": b_ms,
             "sequential_ms_per_step": s_ms, "speedup_vs_sequential": s_ms / b_ms,
+            "sequential_plain_ms_per_step": p_ms,
+            "speedup_vs_plain_per_galaxy_launches": p_ms / b_ms,
             "batched_gpairs_per_s": pairs / (b_ms * 1e-3) / 1e9,
             "frac_fp32_peak": pairs / (b_ms * 1e-3) * 20 / 1e12 / _fp32_peak_tflops(),
             "tuning": res["batched"]["tuning"]}
@@ -190,6 +200,8 @@ def main(argv):
     try:
         from rrgsim_b200 import adjoint
         forms["adjoint"] = adjoint.bench_form
+        forms["adjoint_pm"] = adjoint.bench_form_pm
+        forms["vjp"] = adjoint.bench_form_vjp
     except ImportError:
         pass
     for name, f in forms.items():

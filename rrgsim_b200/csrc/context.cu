@@ -100,6 +100,7 @@ struct rrg_ctx {
     bool soft_uniform = true;
     double uniform_hsoft = 0.0;
     double mass_max = 0.0;
+    double uniform_mass = -1.0;  // >= 0 when every particle has this mass
     bool sorted = false;
     int splits = 1;
     Buf scratch;
@@ -130,7 +131,10 @@ struct rrg_ctx {
     rrg_sim_params sim{};
     double time = 0.0;
     uint64_t iter = 0;
-    int sort_interval = 0;
+    int sort_interval = -1;          // -1: the strategy's default (64 steps in wave mode)
+    int64_t steps_since_sort = INT64_MAX / 2;
+    Buf sort_keys, sort_dest, sort_counts, sort_offsets, sort_cursor, sort_temp, sort_stage;
+    size_t sort_temp_bytes = 0;
     std::map<std::tuple<int, int, int, int>, GraphExec> graphs;
 
     ~rrg_ctx() {
@@ -215,6 +219,7 @@ void direct(rrg_ctx* c, bool want_pot, const DirectEpi& epi) {
     L.poslo = c->L();
     L.hsoft = c->H();
     L.uniform_hsoft = c->uniform_hsoft;
+    L.uniform_mass = c->uniform_mass;
     L.n = c->n;
     L.want_pot = want_pot;
     L.epi = epi;
@@ -321,6 +326,54 @@ void deposit_operator(rrg_ctx* c) {
     launch_cic_deposit(c->prec, c->n, c->P(), c->L(), c->gdev, c->shift_s,
                        c->mg[c->mg_cur].as<unsigned long long>(), c->stream);
     c->src_dirty = true;
+}
+
+// Counting sort of the synced particle state by CIC base cell. Every array is scattered into a
+// staging buffer and copied back in place, so buffer addresses (and recorded graphs) stay.
+void sort_particles(rrg_ctx* c) {
+    require_particles(c);
+    require_grid(c);
+    const int64_t n = c->n;
+    const int64_t nc = static_cast<int64_t>(c->grid.nx) * c->grid.nx * c->grid.nx;
+    if (c->sort_keys.bytes < 4 * static_cast<size_t>(n)) {
+        c->sort_keys.alloc(4 * n);
+        c->sort_dest.alloc(4 * n);
+        c->sort_stage.alloc(v4b(c) * n);
+    }
+    if (c->sort_counts.bytes < 4 * static_cast<size_t>(nc + 1)) {
+        c->sort_counts.alloc(4 * (nc + 1));
+        c->sort_offsets.alloc(4 * (nc + 1));
+        c->sort_cursor.alloc(4 * (nc + 1));
+        c->sort_temp_bytes = sort_scan_temp_bytes(nc);
+        c->sort_temp.alloc(std::max<size_t>(c->sort_temp_bytes, 256));
+    }
+    if (!c->sorted) {
+        c->id.alloc(4 * n);
+        launch_iota(n, c->id.as<int32_t>(), c->stream);
+    }
+    RRG_CUDA(cudaMemsetAsync(c->sort_counts.p, 0, c->sort_counts.bytes, c->stream));
+    RRG_CUDA(cudaMemsetAsync(c->sort_cursor.p, 0, c->sort_cursor.bytes, c->stream));
+    launch_cell_keys(c->prec, n, c->P(), c->L(), c->gdev, c->sort_keys.as<uint32_t>(),
+                     c->sort_counts.as<uint32_t>(), c->stream);
+    launch_scan_counts(c->sort_counts.as<uint32_t>(), c->sort_offsets.as<uint32_t>(), nc,
+                       c->sort_temp.p, c->sort_temp_bytes, c->stream);
+    launch_sort_dest(n, c->sort_keys.as<uint32_t>(), c->sort_offsets.as<uint32_t>(),
+                     c->sort_cursor.as<uint32_t>(), c->sort_dest.as<uint32_t>(), c->stream);
+    auto permute = [&](void* arr, size_t elem) {
+        if (!arr) return;
+        launch_permute(n, elem, c->sort_dest.as<uint32_t>(), arr, c->sort_stage.p, c->stream);
+        RRG_CUDA(cudaMemcpyAsync(arr, c->sort_stage.p, elem * n, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    };
+    permute(c->P(), v4b(c));
+    if (c->prec == RRG_PREC_MIXED) permute(c->L(), sizeof(V4<float>));
+    permute(c->vel.p, v4b(c));
+    permute(c->acc.p, v4b(c));
+    permute(c->pot.p, c->rsz);
+    if (!c->soft_uniform) permute(c->hsoft.p, c->rsz);
+    permute(c->id.p, 4);
+    c->sorted = true;
+    c->steps_since_sort = 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -531,6 +584,9 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         }
         bool uniform = true;
         for (int64_t i = 1; i < n && uniform; ++i) uniform = (soft2[i] == soft2[0]);
+        bool umass = true;
+        for (int64_t i = 1; i < n && umass; ++i) umass = (mass[i] == mass[0]);
+        ctx->uniform_mass = umass ? mass[0] : -1.0;
 
         // recorded graphs stay valid when the new particles reuse every buffer and launch value
         const auto layout = [&]() {
@@ -574,6 +630,7 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         if (!uniform) ctx->hsoft.alloc(ctx->rsz * n);
         else ctx->hsoft.release();
         ctx->id.release();
+        ctx->steps_since_sort = INT64_MAX / 2;
         ctx->splits = direct_choose_splits(ctx->prec, n, ctx->sms);
         const size_t sb = direct_scratch_bytes(ctx->prec, n, ctx->splits);
         if (sb) ctx->scratch.alloc(sb);
@@ -962,11 +1019,20 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
                     RRG_CUDA(cudaMemsetAsync(ctx->mg[1 - ctx->mg_cur].p, 0,
                                              ctx->mg[1 - ctx->mg_cur].bytes, ctx->stream));
                 }
-                // long runs are recorded once per chunk length and replayed
+                // long runs are recorded once per chunk length and replayed; in wave mode the
+                // particles are re-sorted by cell between chunks every sort_interval steps
+                const int interval =
+                    ctx->wave_mode ? (ctx->sort_interval < 0 ? 64 : ctx->sort_interval) : 0;
                 int left = nsteps;
                 while (left > 0) {
-                    const int chunk = std::min(left, 64);
+                    int chunk = std::min(left, 64);
+                    if (interval > 0) {
+                        if (ctx->steps_since_sort >= interval) sort_particles(ctx);
+                        chunk = static_cast<int>(
+                            std::min<int64_t>(chunk, interval - ctx->steps_since_sort));
+                    }
                     run_graph(ctx, chunk);
+                    ctx->steps_since_sort += chunk;
                     left -= chunk;
                 }
             }
@@ -993,6 +1059,19 @@ RRG_API rrg_status rrg_solver_sync(rrg_ctx* ctx) {
             e.acc = ctx->dl.p;
             e.pot = ctx->pot.p;
             direct(ctx, true, e);
+            if (ctx->has_grid) {
+                // rrgsim_integration_nbody.cuh:32-48: CIC mass, then NGP cell averages of the
+                // particle potential and acceleration; the cell counts live in the (unused in
+                // this strategy) source buffer
+                deposit_operator(ctx);
+                RRG_CUDA(cudaMemsetAsync(ctx->src.p, 0, ctx->src.bytes, ctx->stream));
+                RRG_CUDA(cudaMemsetAsync(ctx->phi[ctx->phi_cur].p, 0,
+                                         ctx->phi[ctx->phi_cur].bytes, ctx->stream));
+                RRG_CUDA(cudaMemsetAsync(ctx->acc4.p, 0, ctx->acc4.bytes, ctx->stream));
+                launch_ngp_project(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->gdev,
+                                   ctx->src.as<int>(), ctx->pot.p, ctx->acc.p,
+                                   ctx->phi[ctx->phi_cur].p, ctx->acc4.p, ctx->stream);
+            }
         }
     })
 }

@@ -70,7 +70,10 @@ __device__ __forceinline__ void apply_epi(const EpiDev<R>& e, int64_t i, R ax, R
         e.acc[i] = v4<R>(ax, ay, az, R(0));
         return;
     }
-    // EPI_CORRECT_PREDICT: next step's predict on the corrected velocity.
+    // EPI_CORRECT_PREDICT: next step's predict on the corrected velocity; the synced (v, a)
+    // of this step are stored too where the caller asks (checkpoints)
+    if (e.vel) e.vel[i] = v4<R>(vx, vy, vz, R(0));
+    if (e.acc) e.acc[i] = v4<R>(ax, ay, az, R(0));
     const R sx = vx + dt * ax, sy = vy + dt * ay, sz = vz + dt * az;  // v*
     const R ux = vx + sx, uy = vy + sy, uz = vz + sz;
     e.u[i] = v4<R>(ux, uy, uz, R(0));
@@ -94,6 +97,7 @@ struct F32Params {
     const V4<float>* poslo;
     const float* hsoft;
     float uniform_h;
+    float uniform_m;     // every particle's mass when all are equal (UMASS kernels)
     int64_t n;
     int64_t jchunk;
     V4<float>* part_hi;  // [splits][n]
@@ -248,7 +252,10 @@ __global__ void __launch_bounds__(kBS, 2) direct_f32_kernel(const F32Params p) {
 // lands directly in the register pairs the paired instructions read. Same arithmetic per pair
 // as direct_f32_kernel (FP32 mode, tile-blocked summation).
 // ----------------------------------------------------------------------------------------------
-template <int G, bool USOFT, bool POT>
+// UMASS: every particle has the mass p.uniform_m, which then multiplies the sums once at the
+// end instead of every pair (11 FP32 operations per pair instead of 12). The massless padding
+// of a last tile sits 1e18 away: its inv^3 flushes to zero and its inv adds below 1e-18.
+template <int G, bool USOFT, bool POT, bool UMASS>
 __global__ void __launch_bounds__(kBS, 2) direct_f32x2_kernel(const F32Params p) {
     __shared__ float4 s_xy[kBS];
     __shared__ float4 s_zm[kBS];
@@ -330,7 +337,7 @@ __global__ void __launch_bounds__(kBS, 2) direct_f32x2_kernel(const F32Params p)
                 const float2 s = USOFT ? hs[g] : __fadd2_rn(hs[g], hj);
                 const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, s)));
                 const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
-                const float2 minv = __fmul2_rn(pm, inv);
+                const float2 minv = UMASS ? inv : __fmul2_rn(pm, inv);
                 const float2 kk = __fmul2_rn(minv, __fmul2_rn(inv, inv));
                 tx[g] = __ffma2_rn(dx, kk, tx[g]);
                 ty[g] = __ffma2_rn(dy, kk, ty[g]);
@@ -352,8 +359,14 @@ __global__ void __launch_bounds__(kBS, 2) direct_f32x2_kernel(const F32Params p)
         for (int e = 0; e < 2; ++e) {
             const int64_t i = ibase + (2 * g + e) * kBS + tid;
             if (i >= n) continue;
-            const float fx = e ? ax[g].y : ax[g].x, fy = e ? ay[g].y : ay[g].x,
-                        fz = e ? az[g].y : az[g].x, fp = e ? ap[g].y : ap[g].x;
+            float fx = e ? ax[g].y : ax[g].x, fy = e ? ay[g].y : ay[g].x,
+                  fz = e ? az[g].y : az[g].x, fp = e ? ap[g].y : ap[g].x;
+            if constexpr (UMASS) {
+                fx *= p.uniform_m;
+                fy *= p.uniform_m;
+                fz *= p.uniform_m;
+                fp *= p.uniform_m;
+            }
             if (gridDim.y > 1) {
                 p.part_hi[static_cast<int64_t>(blockIdx.y) * n + i] = v4<float>(fx, fy, fz, fp);
             } else {
@@ -512,8 +525,8 @@ int resident_blocks(int prec, int variant) {
                          : reinterpret_cast<const void*>(&direct_f32_kernel<2, true, true, false>);
     else if (variant == 1) k = reinterpret_cast<const void*>(&direct_f32_kernel<1, true, false, false>);
     else if (variant == 2) k = reinterpret_cast<const void*>(&direct_f32_kernel<2, true, false, false>);
-    else if (variant == 3) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<1, true, false>);
-    else k = reinterpret_cast<const void*>(&direct_f32x2_kernel<2, true, false>);
+    else if (variant == 3) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<1, true, false, false>);
+    else k = reinterpret_cast<const void*>(&direct_f32x2_kernel<2, true, false, false>);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kBS, 0) != cudaSuccess || nb < 1) {
         (void)cudaGetLastError();
@@ -527,7 +540,9 @@ int resident_blocks(int prec, int variant) {
 
 // j-split count: the smallest one whose block count fills whole waves of resident blocks to
 // within 2% of the best achievable (wave quantisation is what costs at these sizes; each
-// extra split only adds n x 16 B of partials and a tiny reduction).
+// extra split only adds n x 16 B of partials and a tiny reduction). The count is a request:
+// the launch rounds it to whole j-tile chunks, and on B200 that measured faster at N = 16,384
+// than choosing among realisable counts only.
 int direct_choose_splits(int prec, int64_t n, int sms) {
     const int variant = variant_for(prec, n);
     const int ipt = ipt_of(variant);
@@ -566,7 +581,10 @@ void launch_direct(const DirectLaunch& L) {
     RRG_REQUIRE(real_splits <= 1 || L.scratch_bytes >= direct_scratch_bytes(L.prec, L.n, real_splits),
                 RRG_ERR_INVALID, "direct sum: scratch too small for the split count");
     const bool usoft = (L.hsoft == nullptr);
-    const int ipt = ipt_for(L.prec, L.n);
+    const int variant = (L.prec == RRG_PREC_FP32 && L.variant >= 1 && L.variant <= 4)
+                            ? L.variant
+                            : variant_for(L.prec, L.n);
+    const int ipt = L.prec == RRG_PREC_FP64 ? 1 : ipt_of(variant);
 
     if (L.prec == RRG_PREC_FP64) {
         F64Params p;
@@ -611,21 +629,27 @@ void launch_direct(const DirectLaunch& L) {
     RRG_REQUIRE(!mixed || L.poslo != nullptr, RRG_ERR_INVALID,
                 "direct sum: MIXED precision needs the low position parts");
     dim3 grid(static_cast<unsigned>((L.n + kBS * ipt - 1) / (kBS * ipt)), real_splits);
-    const int variant = variant_for(L.prec, L.n);
     if (variant >= 3) {
-#define RRG_X2(G)                                                                              \
-    do {                                                                                       \
-        if (usoft) {                                                                           \
-            if (L.want_pot) direct_f32x2_kernel<G, true, true><<<grid, kBS, 0, L.stream>>>(p); \
-            else direct_f32x2_kernel<G, true, false><<<grid, kBS, 0, L.stream>>>(p);           \
-        } else {                                                                               \
-            if (L.want_pot) direct_f32x2_kernel<G, false, true><<<grid, kBS, 0, L.stream>>>(p);\
-            else direct_f32x2_kernel<G, false, false><<<grid, kBS, 0, L.stream>>>(p);          \
-        }                                                                                      \
+        const bool umass = L.uniform_mass >= 0.0;
+        p.uniform_m = umass ? static_cast<float>(L.uniform_mass) : 0.f;
+#define RRG_X2M(G, M)                                                                            \
+    do {                                                                                         \
+        if (usoft) {                                                                             \
+            if (L.want_pot) direct_f32x2_kernel<G, true, true, M><<<grid, kBS, 0, L.stream>>>(p); \
+            else direct_f32x2_kernel<G, true, false, M><<<grid, kBS, 0, L.stream>>>(p);          \
+        } else {                                                                                 \
+            if (L.want_pot) direct_f32x2_kernel<G, false, true, M><<<grid, kBS, 0, L.stream>>>(p);\
+            else direct_f32x2_kernel<G, false, false, M><<<grid, kBS, 0, L.stream>>>(p);         \
+        }                                                                                        \
     } while (0)
-        if (variant == 3) RRG_X2(1);
-        else RRG_X2(2);
-#undef RRG_X2
+        if (variant == 3) {
+            if (umass) RRG_X2M(1, true);
+            else RRG_X2M(1, false);
+        } else {
+            if (umass) RRG_X2M(2, true);
+            else RRG_X2M(2, false);
+        }
+#undef RRG_X2M
     } else if (ipt == 1) {
         dispatch_f32<1>(usoft, mixed, L.want_pot, grid, p, L.stream);
     } else {

@@ -28,7 +28,7 @@ struct EnsGalaxy {
     int32_t n;
     int32_t splits;
     float h2;          // soft2 of the galaxy (h_i + h_j)
-    float pad;
+    float m;           // particle mass when every particle of the ensemble galaxy has one
 };
 
 struct EnsItem {
@@ -46,7 +46,8 @@ struct EnsForceParams {
 
 // Persistent force kernel: G float2 groups per thread (2 G i-particles), paired FP32 ops as
 // in direct_f32x2_kernel.
-template <int G>
+// UMASS: all particles of each galaxy share its mass gg.m (multiplied in once per sum).
+template <int G, bool UMASS>
 __global__ void __launch_bounds__(kBS, 2) ens_forces_kernel(const EnsForceParams p) {
     __shared__ float4 s_xy[kBS];
     __shared__ float4 s_zm[kBS];
@@ -108,7 +109,8 @@ __global__ void __launch_bounds__(kBS, 2) ens_forces_kernel(const EnsForceParams
                     const float2 r2 =
                         __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, hs)));
                     const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
-                    const float2 kk = __fmul2_rn(__fmul2_rn(pm, inv), __fmul2_rn(inv, inv));
+                    const float2 minv = UMASS ? inv : __fmul2_rn(pm, inv);
+                    const float2 kk = __fmul2_rn(minv, __fmul2_rn(inv, inv));
                     tx[g] = __ffma2_rn(dx, kk, tx[g]);
                     ty[g] = __ffma2_rn(dy, kk, ty[g]);
                     tz[g] = __ffma2_rn(dz, kk, tz[g]);
@@ -127,9 +129,10 @@ __global__ void __launch_bounds__(kBS, 2) ens_forces_kernel(const EnsForceParams
             for (int e = 0; e < 2; ++e) {
                 const int li = w.i0 + (2 * g + e) * kBS + tid;
                 if (li >= gg.n) continue;
+                const float sc = UMASS ? gg.m : 1.f;
                 p.part[gg.part_off + static_cast<int64_t>(w.s) * gg.n + li] =
-                    v4<float>(e ? ax[g].y : ax[g].x, e ? ay[g].y : ay[g].x,
-                              e ? az[g].y : az[g].x, 0.f);
+                    v4<float>(sc * (e ? ax[g].y : ax[g].x), sc * (e ? ay[g].y : ay[g].x),
+                              sc * (e ? az[g].y : az[g].x), 0.f);
             }
         }
     }
@@ -240,6 +243,8 @@ struct rrg_ensemble {
     double dt = 0.0;
     std::vector<int64_t> counts, offs;
     std::vector<float> h2;
+    std::vector<float> gmass;  // per-galaxy particle mass (all equal within every galaxy)
+    bool umass = false;
     DevBuf posm[2], vel, acc, u, gid, gal, items, part, counter;
     int cur = 0;
     int variant = 1;      // 1: G = 1 (2 i per thread), 2: G = 2 (4 i per thread)
@@ -275,7 +280,7 @@ void build_worklist(rrg_ensemble* e, int variant, int jchunk) {
     for (int g = 0; g < e->ngal; ++g) {
         const int n = static_cast<int>(e->counts[g]);
         const int splits = (n + jchunk - 1) / jchunk;
-        gal[g] = EnsGalaxy{e->offs[g], part_off, n, splits, e->h2[g], 0.f};
+        gal[g] = EnsGalaxy{e->offs[g], part_off, n, splits, e->h2[g], e->gmass[g]};
         part_off += static_cast<int64_t>(splits) * n;
         for (int i0 = 0; i0 < n; i0 += itile)
             for (int s = 0; s < splits; ++s)
@@ -298,9 +303,9 @@ void build_worklist(rrg_ensemble* e, int variant, int jchunk) {
     e->jchunk = jchunk;
     int nb = 0;
     if (variant == 2)
-        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ens_forces_kernel<2>, kBS, 0));
+        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ens_forces_kernel<2, false>, kBS, 0));
     else
-        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ens_forces_kernel<1>, kBS, 0));
+        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ens_forces_kernel<1, false>, kBS, 0));
     e->grid = std::min(num_sms(e->device) * std::max(nb, 1), std::max(e->num_items, 1));
     drop_ens_graphs(e);
 }
@@ -314,8 +319,13 @@ void launch_forces(rrg_ensemble* e, const void* posm) {
     p.num_items = e->num_items;
     p.counter = e->counter.as<unsigned int>();
     p.part = e->part.as<V4<float>>();
-    if (e->variant == 2) ens_forces_kernel<2><<<e->grid, kBS, 0, e->stream>>>(p);
-    else ens_forces_kernel<1><<<e->grid, kBS, 0, e->stream>>>(p);
+    if (e->umass) {
+        if (e->variant == 2) ens_forces_kernel<2, true><<<e->grid, kBS, 0, e->stream>>>(p);
+        else ens_forces_kernel<1, true><<<e->grid, kBS, 0, e->stream>>>(p);
+    } else {
+        if (e->variant == 2) ens_forces_kernel<2, false><<<e->grid, kBS, 0, e->stream>>>(p);
+        else ens_forces_kernel<1, false><<<e->grid, kBS, 0, e->stream>>>(p);
+    }
     RRG_LAUNCHED();
 }
 
@@ -458,6 +468,7 @@ RRG_API rrg_status rrg_ensemble_create(int device, int ngal, const int64_t* coun
             e->counts.push_back(counts[g]);
             e->offs.push_back(tot);
             e->h2.push_back(static_cast<float>(soft2_per_galaxy[g]));
+            e->gmass.push_back(static_cast<float>(mass[tot]));
             tot += counts[g];
         }
         RRG_REQUIRE(tot < (int64_t(1) << 31), RRG_ERR_INVALID,
@@ -466,6 +477,11 @@ RRG_API rrg_status rrg_ensemble_create(int device, int ngal, const int64_t* coun
             RRG_REQUIRE(std::isfinite(pos[i]) && std::isfinite(vel[i]), RRG_ERR_INVALID,
                         "rrg_ensemble_create: non-finite position or velocity");
         e->ntot = tot;
+        // equal masses within every galaxy: the paired kernel folds the mass out of the pair
+        e->umass = true;
+        for (int g = 0; g < ngal && e->umass; ++g)
+            for (int64_t k = 1; k < counts[g] && e->umass; ++k)
+                e->umass = mass[e->offs[g] + k] == mass[e->offs[g]];
         RRG_CUDA(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
         e->stream = e->own;
         const size_t vb = sizeof(V4<float>) * tot;
@@ -532,8 +548,10 @@ RRG_API rrg_status rrg_ensemble_step(rrg_ensemble* e, int nsteps) {
     })
 }
 
-// Per-galaxy launches of the same force kernel (no batching): the comparison baseline.
-RRG_API rrg_status rrg_ensemble_step_sequential(rrg_ensemble* e, int nsteps) {
+// One force launch per galaxy (no batching): the comparison baseline. plain != 0 uses the
+// reference's launch shape (one i-particle per thread, 256-thread blocks, no j-split, scalar
+// FP32 pairs); plain == 0 the library's own single-galaxy kernel without a j-split.
+RRG_API rrg_status rrg_ensemble_step_sequential(rrg_ensemble* e, int nsteps, int plain) {
     ENS_ENTRY(e, {
         RRG_REQUIRE(nsteps >= 0, RRG_ERR_INVALID, "nsteps must be >= 0");
         for (int s = 0; s < nsteps; ++s) {
@@ -552,7 +570,8 @@ RRG_API rrg_status rrg_ensemble_step_sequential(rrg_ensemble* e, int nsteps) {
                 L.epi.vel = e->vel.as<V4<float>>() + e->offs[g];
                 L.epi.acc = e->acc.as<V4<float>>() + e->offs[g];
                 L.epi.u = e->u.as<V4<float>>() + e->offs[g];
-                L.splits = 1;  // one plain launch per galaxy
+                L.splits = 1;  // one launch per galaxy
+                L.variant = plain ? 1 : 0;
                 L.stream = e->stream;
                 launch_direct(L);
             }

@@ -108,13 +108,16 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
     }
 }
 
+// One warp per reduced value: lane l sums blocks l, l + 32, ... in order, then a fixed
+// shuffle tree (deterministic).
 __global__ void conservation_finish(const double* __restrict__ partial, int nblocks,
                                     double* __restrict__ out) {
-    const int k = threadIdx.x;
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (k >= kRedVals) return;
     double t = 0.0;
-    for (int b = 0; b < nblocks; ++b) t += partial[static_cast<int64_t>(b) * kRedVals + k];
-    out[k] = t;
+    for (int b = lane; b < nblocks; b += 32) t += partial[static_cast<int64_t>(b) * kRedVals + k];
+    t = warp_sum(t);
+    if (lane == 0) out[k] = t;
 }
 
 // Host FP64 AoS -> device state.
@@ -236,7 +239,7 @@ void launch_conservation(int prec, int64_t n, const void* posm, const void* posl
             n, static_cast<const V4<float>*>(posm), nullptr, static_cast<const V4<float>*>(vel),
             static_cast<const float*>(pot), partial);
     RRG_LAUNCHED();
-    conservation_finish<<<1, 32, 0, s>>>(partial, nblocks, out);
+    conservation_finish<<<1, 32 * kRedVals, 0, s>>>(partial, nblocks, out);
     RRG_LAUNCHED();
 }
 

@@ -13,6 +13,7 @@ enum DirectEpiMode {
     EPI_STORE = 0,            // acc[i] = a (and pot[i] = phi when requested)
     EPI_CORRECT = 1,          // v = (u + dt a) / 2 -> vel; acc[i] = a
     EPI_CORRECT_PREDICT = 2,  // v as above, then u' = v + (v + dt a), x' = x + dt/2 u' -> pos_out
+                              // (v and a stored as well where vel / acc are non-null)
 };
 
 struct DirectEpi {
@@ -32,10 +33,12 @@ struct DirectLaunch {
     const void* poslo = nullptr;  // V4<float> (MIXED only)
     const void* hsoft = nullptr;  // R[n] soft2/2, or nullptr -> uniform_hsoft
     double uniform_hsoft = 0.0;
+    double uniform_mass = -1.0;   // >= 0: every particle has this mass (FP32 paired kernels)
     int64_t n = 0;
     bool want_pot = false;
     DirectEpi epi;
     int splits = 0;               // j-splits; 0 = choose
+    int variant = 0;              // FP32 kernel variant (direct.cu); 0 = choose
     void* scratch = nullptr;      // partial sums when splits > 1
     size_t scratch_bytes = 0;
     cudaStream_t stream = nullptr;
@@ -112,6 +115,13 @@ void launch_interp(int prec, int64_t n, const void* posm, const void* poslo, con
 void launch_ngp_phi(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
                     const void* phi, void* pot, cudaStream_t s);
 
+// NGP averages of particle potential / acceleration per cell (rm_p2mesh.cu:142-174):
+// count[] (nx^3 ints, zeroed by the caller) receives the cell counts; phi_grid (R, nx^3) and
+// acc4_grid (V4<R>, nx^3) must be zeroed by the caller; either may be nullptr.
+void launch_ngp_project(int prec, int64_t n, const void* posm, const void* poslo,
+                        const GridDev& g, int* count, const void* pot, const void* acc,
+                        void* phi_grid, void* acc4_grid, cudaStream_t s);
+
 // Fused particle pass of the wave strategy: optional [trilinear interp + correct] then
 // optional [predict + CIC deposit].
 enum PmMode { PM_INTERP_CORRECT = 1, PM_PREDICT_DEPOSIT = 2, PM_WRITE_SYNC = 4 };
@@ -131,26 +141,17 @@ struct PmParticleArgs {
 };
 void launch_pm_particles(const PmParticleArgs& a, int mode, cudaStream_t s);
 
-// Counting sort by NGP cell: keys, histogram, scan, scatter of the particle arrays.
-struct SortArgs {
-    int prec;
-    int64_t n;
-    GridDev g;
-    // arrays permuted (in -> out); any may be nullptr
-    const void* posm; void* posm_out;
-    const void* poslo; void* poslo_out;
-    const void* vel; void* vel_out;
-    const void* acc; void* acc_out;
-    const void* u; void* u_out;
-    const void* hsoft; void* hsoft_out;
-    const int32_t* id; int32_t* id_out;
-    // scratch
-    uint32_t* keys;      // n
-    uint32_t* counts;    // nx^3 + 1
-    uint32_t* offsets;   // nx^3 + 1
-    uint32_t* block_sums;  // scan block partials
-};
-size_t sort_scan_blocks(int ncells);
-void launch_sort_by_cell(const SortArgs& a, cudaStream_t s);
+// Counting sort by CIC base cell (sort.cu): keys + histogram, exclusive scan, destinations,
+// then one scatter per particle array.
+size_t sort_scan_temp_bytes(int64_t ncells);
+void launch_cell_keys(int prec, int64_t n, const void* posm, const void* poslo,
+                      const GridDev& g, uint32_t* keys, uint32_t* counts, cudaStream_t s);
+void launch_scan_counts(const uint32_t* counts, uint32_t* offsets, int64_t ncells, void* temp,
+                        size_t temp_bytes, cudaStream_t s);
+void launch_sort_dest(int64_t n, const uint32_t* keys, const uint32_t* offsets,
+                      uint32_t* cursor, uint32_t* dest, cudaStream_t s);
+void launch_permute(int64_t n, size_t elem_bytes, const uint32_t* dest, const void* in,
+                    void* out, cudaStream_t s);
+void launch_iota(int64_t n, int32_t* id, cudaStream_t s);
 
 }  // namespace rrg

@@ -211,8 +211,86 @@ __device__ __forceinline__ unsigned long long dbits(double v) {
     return static_cast<unsigned long long>(__double_as_longlong(v));
 }
 
+// Block-wide max of (dmax, amax) folded into maxbits[0..1] (non-negative doubles compare as
+// their bit patterns).
+__device__ __forceinline__ void block_max_to(double dmax, double amax, int tid,
+                                             unsigned long long* maxbits) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, o));
+        amax = fmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+    }
+    __shared__ double sd[kTX * kTY / 32], sa[kTX * kTY / 32];
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) {
+        sd[wid] = dmax;
+        sa[wid] = amax;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double d = 0, a = 0;
+        for (int k = 0; k < kTX * kTY / 32; ++k) {
+            d = fmax(d, sd[k]);
+            a = fmax(a, sa[k]);
+        }
+        atomicMax(maxbits, dbits(d));
+        atomicMax(maxbits + 1, dbits(a));
+    }
+}
+
+// Periodic box without an absorbing layer (the reference's wired path, wave.cu:177-181):
+// constant coefficients, wrapped neighbours, and a compile-time z-chunk so the column's
+// ZC + 2 potential values are all requested before the first update (memory-level
+// parallelism for a latency-bound stencil).
+template <typename R, int ZC, bool CHECK>
+__global__ void __launch_bounds__(kTX* kTY, 8) wave_periodic_kernel(
+    const R* __restrict__ phi, R* __restrict__ phi_old, const R* __restrict__ src,
+    const WaveDev w, unsigned long long* __restrict__ maxbits) {
+    const int nx = w.nx;
+    const int plane = nx * nx;
+    const int tid = threadIdx.y * kTX + threadIdx.x;
+    const int x = blockIdx.x * kTX + threadIdx.x;
+    const int y = blockIdx.y * kTY + threadIdx.y;
+    double dmax = 0.0, amax = 0.0;
+    if (x < nx && y < nx) {
+        const int oxm = x > 0 ? -1 : nx - 1;
+        const int oxp = x < nx - 1 ? 1 : -(nx - 1);
+        const int oym = y > 0 ? -nx : (nx - 1) * nx;
+        const int oyp = y < nx - 1 ? nx : -(nx - 1) * nx;
+        const int col = x + y * nx;
+        const int z0 = blockIdx.z * ZC;
+        const R km = static_cast<R>(w.K_MAIN), ka = static_cast<R>(w.K_ACTUAL),
+                ko = static_cast<R>(w.K_OLD), kf = static_cast<R>(w.K_F);
+        R pv[ZC + 2];  // phi at z0 - 1 ... z0 + ZC (wrapped)
+#pragma unroll
+        for (int k = 0; k < ZC + 2; ++k) {
+            int z = z0 - 1 + k;
+            z = z < 0 ? z + nx : (z >= nx ? z - nx : z);
+            pv[k] = __ldg(phi + col + z * plane);
+        }
+#pragma unroll
+        for (int k = 0; k < ZC; ++k) {
+            const int z = z0 + k;
+            if (z < nx) {
+                const int c = col + z * plane;
+                const R lap = __ldg(phi + c + oxm) + __ldg(phi + c + oxp) +
+                              __ldg(phi + c + oym) + __ldg(phi + c + oyp) + pv[k] + pv[k + 2];
+                const R out = lap * km + pv[k + 1] * ka + phi_old[c] * ko + src[c] * kf;
+                phi_old[c] = out;
+                if constexpr (CHECK) {
+                    dmax = fmax(dmax, fabs(static_cast<double>(out) - static_cast<double>(pv[k + 1])));
+                    amax = fmax(amax, fabs(static_cast<double>(out)));
+                }
+            }
+        }
+    }
+    if constexpr (CHECK) block_max_to(dmax, amax, tid, maxbits);
+}
+
+// UNIFORM is the periodic box without an absorbing layer (the reference's wired path): the
+// boundary code compiles away and the kernel fits 8 resident blocks per SM.
 template <typename R, bool UNIFORM, bool CHECK>
-__global__ void __launch_bounds__(kTX* kTY) wave_step_kernel(
+__global__ void __launch_bounds__(kTX* kTY, UNIFORM ? 8 : 2) wave_step_kernel(
     const R* __restrict__ phi, R* __restrict__ phi_old, const R* __restrict__ src,
     const WaveDev w, unsigned long long* __restrict__ maxbits) {
     // One thread per (x, y) column marches through zc planes: phi(z - 1), phi(z), phi(z + 1)
@@ -224,7 +302,7 @@ __global__ void __launch_bounds__(kTX* kTY) wave_step_kernel(
     const int x = blockIdx.x * kTX + threadIdx.x;
     const int y = blockIdx.y * kTY + threadIdx.y;
     const bool valid = (x < nx) && (y < nx);
-    const bool periodic = (w.bc == RRG_BC_PERIODIC);
+    const bool periodic = UNIFORM ? true : (w.bc == RRG_BC_PERIODIC);
     double dmax = 0.0, amax = 0.0;
     if (valid) {
         // in-plane neighbour offsets: periodic wrap, or clamped (unused on the boundary nodes)
@@ -425,6 +503,52 @@ __global__ void __launch_bounds__(256) ngp_phi_kernel(int64_t n, const void* __r
 }
 
 // ----------------------------------------------------------------------------------------------
+// NGP projections of particle values onto the grid (N-body strategy with a grid,
+// rrgsim_integration_nbody.cuh:32-48): per-cell particle counts (assign_particles_to_cells_,
+// rm_p2mesh.cu:25-66), then each particle adds value / count of its cell
+// (deposit_cell_grav_NGP_ / deposit_cell_acc_NGP_, rm_p2mesh.cu:142-174).
+template <typename R>
+__device__ __forceinline__ int64_t ngp_cell(const void* posm, const V4<float>* lo, int64_t i,
+                                            const GridDev& g) {
+    double x, y, z, m;
+    load_pos<R>(posm, lo, i, x, y, z, m);
+    const int64_t nx = g.nx;
+    return ngp_axis(x, g.domain_min, g.dx, g.nx) + ngp_axis(y, g.domain_min, g.dx, g.nx) * nx +
+           ngp_axis(z, g.domain_min, g.dx, g.nx) * nx * nx;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) ngp_count_kernel(int64_t n, const void* __restrict__ posm,
+                                                        const V4<float>* __restrict__ lo,
+                                                        GridDev g, int* __restrict__ count) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    atomicAdd(count + ngp_cell<R>(posm, lo, i, g), 1);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) ngp_project_kernel(int64_t n, const void* __restrict__ posm,
+                                                          const V4<float>* __restrict__ lo,
+                                                          GridDev g, const int* __restrict__ count,
+                                                          const R* __restrict__ pot,
+                                                          const V4<R>* __restrict__ acc,
+                                                          R* __restrict__ phi_grid,
+                                                          R* __restrict__ acc_grid) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t c = ngp_cell<R>(posm, lo, i, g);
+    const R cnt = static_cast<R>(count[c]);
+    if (phi_grid) atomicAdd(phi_grid + c, pot[i] / cnt);
+    if (acc_grid) {
+        const V4<R> a = acc[i];
+        const R inv = R(1) / cnt;
+        atomicAdd(acc_grid + 4 * c, a.x * inv);
+        atomicAdd(acc_grid + 4 * c + 1, a.y * inv);
+        atomicAdd(acc_grid + 4 * c + 2, a.z * inv);
+    }
+}
+
+// ----------------------------------------------------------------------------------------------
 // Fused particle pass of the wave strategy (one launch per step):
 //   [INTERP_CORRECT]  a = trilinear(x); v = (u + dt a) / 2                  (correct_step_)
 //   [PREDICT_DEPOSIT] v* = v + dt a; u = v + v*; x += dt/2 u; CIC(x)        (predict_step_ +
@@ -593,6 +717,31 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
     dim3 grid(gx, gy, div_up(nx, zc));
     dim3 block(kTX, kTY);
     const bool check = maxbits != nullptr;
+    if (w.uniform) {
+        // compile-time chunk of 2, 4 or 8 planes, the nearest the chooser's pick
+        const int zcf = zc >= 8 ? 8 : (zc >= 4 ? 4 : 2);
+        dim3 g2(gx, gy, div_up(nx, zcf));
+#define RRG_WAVE_P(R, Z)                                                                      \
+    do {                                                                                      \
+        const R* p = static_cast<const R*>(phi);                                              \
+        R* po = static_cast<R*>(phi_old_inout);                                               \
+        const R* sr = static_cast<const R*>(src);                                             \
+        if (check) wave_periodic_kernel<R, Z, true><<<g2, block, 0, s>>>(p, po, sr, w, maxbits); \
+        else wave_periodic_kernel<R, Z, false><<<g2, block, 0, s>>>(p, po, sr, w, maxbits);      \
+    } while (0)
+        if (prec == RRG_PREC_FP64) {
+            if (zcf == 8) RRG_WAVE_P(double, 8);
+            else if (zcf == 4) RRG_WAVE_P(double, 4);
+            else RRG_WAVE_P(double, 2);
+        } else {
+            if (zcf == 8) RRG_WAVE_P(float, 8);
+            else if (zcf == 4) RRG_WAVE_P(float, 4);
+            else RRG_WAVE_P(float, 2);
+        }
+#undef RRG_WAVE_P
+        RRG_LAUNCHED();
+        return;
+    }
 #define RRG_WAVE_LAUNCH(R)                                                                    \
     do {                                                                                      \
         const R* p = static_cast<const R*>(phi);                                              \
@@ -651,6 +800,29 @@ void launch_ngp_phi(int prec, int64_t n, const void* posm, const void* poslo, co
         ngp_phi_kernel<float><<<b, 256, 0, s>>>(
             n, posm, prec == RRG_PREC_MIXED ? static_cast<const V4<float>*>(poslo) : nullptr, g,
             static_cast<const float*>(phi), static_cast<float*>(pot));
+    RRG_LAUNCHED();
+}
+
+void launch_ngp_project(int prec, int64_t n, const void* posm, const void* poslo,
+                        const GridDev& g, int* count, const void* pot, const void* acc,
+                        void* phi_grid, void* acc4_grid, cudaStream_t s) {
+    const int b = div_up(n, 256);
+    const V4<float>* lo = prec == RRG_PREC_MIXED ? static_cast<const V4<float>*>(poslo) : nullptr;
+    if (prec == RRG_PREC_FP64) {
+        ngp_count_kernel<double><<<b, 256, 0, s>>>(n, posm, nullptr, g, count);
+        RRG_LAUNCHED();
+        ngp_project_kernel<double><<<b, 256, 0, s>>>(
+            n, posm, nullptr, g, count, static_cast<const double*>(pot),
+            static_cast<const V4<double>*>(acc), static_cast<double*>(phi_grid),
+            static_cast<double*>(acc4_grid));
+    } else {
+        ngp_count_kernel<float><<<b, 256, 0, s>>>(n, posm, lo, g, count);
+        RRG_LAUNCHED();
+        ngp_project_kernel<float><<<b, 256, 0, s>>>(
+            n, posm, lo, g, count, static_cast<const float*>(pot),
+            static_cast<const V4<float>*>(acc), static_cast<float*>(phi_grid),
+            static_cast<float*>(acc4_grid));
+    }
     RRG_LAUNCHED();
 }
 

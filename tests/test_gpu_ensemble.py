@@ -46,12 +46,16 @@ def test_ensemble_matches_single_galaxy_contexts_and_oracle(autotune):
         assert np.median(rel_err(got["acc"][sl], ra)) <= 1e-4
 
 
-def test_sequential_baseline_gives_the_same_state():
+@pytest.mark.parametrize("plain", [False, True])
+def test_sequential_baseline_gives_the_same_state(plain):
     counts, pos, vel, mass, s2 = _small_ensemble()
     out = []
     for seq in (False, True):
         with rg.Ensemble(counts, pos, vel, mass, s2, 1e-3, autotune=False) as e:
-            (e.step_sequential if seq else e.step)(5)
+            if seq:
+                e.step_sequential(5, plain=plain)
+            else:
+                e.step(5)
             out.append(e.get())
     np.testing.assert_allclose(out[0]["pos"], out[1]["pos"], rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(out[0]["vel"], out[1]["vel"], rtol=1e-4, atol=1e-5)

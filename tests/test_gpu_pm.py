@@ -244,3 +244,39 @@ def test_sorting_by_cell_changes_nothing_but_memory_order():
         np.testing.assert_array_equal(p0[k], p1[k])
     np.testing.assert_array_equal(g0["mass"], g1["mass"])
     np.testing.assert_array_equal(g0["grav"], g1["grav"])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_nbody_sync_projects_particles_on_grid(prec):
+    """N-body strategy with a grid (rrgsim_integration_nbody.cuh:32-48): the sync deposits the
+    CIC mass and writes NGP cell averages of the particle potential and acceleration."""
+    n, nx, dt = 6000, 16, 1e-3
+    pos, vel, m, s2 = disk(n, seed=21)
+    pos[:3] = [[9.5, 0, 0], [-8.0, -8.0, 8.0], [0.0, 0.0, 0.0]]  # clamped and face cells
+    g = _grid(nx)
+    sim = rg.SimParams(time_max=1.0, dt_save=0.1, dt_dynamics=dt, saves_without_dump=2 ** 63,
+                       use_wave_model=0)
+    with _ctx(prec, pos, vel, m, s2, g) as c:
+        c.solver_init(sim)
+        c.precalc()
+        c.calc_steps(3)
+        c.sync_particles_and_grid()
+        p = c.get_particles()
+        grid = c.get_grid()
+        shift = c.deposit_scale()
+    og = _orc_grid(g)
+    held_m = m if prec == "fp64" else f32(m)
+    held_pos = p["pos"] if prec == "fp64" else f32(p["pos"])
+    q = orc.cic_fixed(held_pos, held_m, og, shift)
+    np.testing.assert_array_equal(grid["mass"], q.astype(np.float64) * 2.0 ** -shift)
+    want_phi = orc.ngp_project(held_pos, og, p["grav"])
+    want_acc = orc.ngp_project(held_pos, og, p["acc"])
+    # cell sums of value / count: the order of the device's atomics only
+    tol = 1e-12 if prec == "fp64" else 2e-6
+    scale_phi = np.max(np.abs(want_phi))
+    scale_acc = np.max(np.abs(want_acc))
+    assert np.max(np.abs(grid["grav"] - want_phi)) <= tol * scale_phi
+    assert np.max(np.abs(grid["acc"] - want_acc)) <= tol * scale_acc
+    occupied = np.bincount(orc.ngp_cell(held_pos, og), minlength=nx ** 3) > 0
+    assert np.all(grid["grav"][~occupied] == 0.0)
+    assert np.all(grid["grav"][occupied] < 0.0)

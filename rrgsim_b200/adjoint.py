@@ -250,7 +250,7 @@ def bench_form(torch_mod=None, n=16384, nsteps=200, dt=1e-3, eps=0.02, every=20,
         grads[prec] = (x0r.grad.double().cpu().numpy(), v0r.grad.double().cpu().numpy(),
                        mr.grad.double().cpu().numpy())
         res[prec] = {"forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
-                     "loss": float(loss)}
+                     "loss": float(loss.detach())}
         if prec == "fp64":
             # central differences along random directions in (x0, v0, m), FP64 forward model
             fd_rel = []
@@ -424,7 +424,7 @@ def bench_form_pm(torch_mod=None, n=262144, nx=64, nsteps=200, dt=2e-3, substeps
         fwd, bwd = e0.elapsed_time(e1), e1.elapsed_time(e2)
         grads[prec] = np.concatenate([a.grad.double().cpu().numpy().ravel() for a in (xr, vr, mr)])
         res[prec] = {"forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
-                     "loss": float(loss)}
+                     "loss": float(loss.detach())}
         if prec == "fp64":
             h = 1e-3
             rel, rel32 = [], []

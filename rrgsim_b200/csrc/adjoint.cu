@@ -20,9 +20,15 @@
 //   c_n = dt^2/2 X + dt/2 V + dt/2 V_n      (the last term: v_n's own dependence on a(x_n),
 //                                             absent for n = 0 where v_0 is an input)
 //   X_n = X + J(x_n)^T c_n,   mbar += (da(x_n)/dm)^T c_n
-// so each step costs one vector-Jacobian product at x_n. States x_n come from checkpoints
-// every K steps (x, v and a(x), so a segment's recompute starts without a force evaluation),
-// recomputed segment by segment: K - 1 force evaluations per K steps.
+// so each step costs one vector-Jacobian product at x_n. The forward keeps (x, v, a(x)) every
+// K steps. Between checkpoints the states come back two ways:
+//   FP64: recomputed forward from the checkpoint below (K - 2 force evaluations per K steps),
+//         so the gradient is the exact adjoint of the forward trajectory;
+//   FP32: the leapfrog run backwards from the checkpoint above (reverse_init_kernel,
+//         vjp_reverse_finish), the force a(x_m) summed in the same pass over the pairs as the
+//         VJP at x_m (3 more operations per pair instead of a separate force evaluation).
+//         Each reversed step rounds once more than the forward did; every segment restarts
+//         from an exact checkpoint.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -47,6 +53,7 @@ struct VjpParams {
     V4<R>* out;
     V4<R>* part;
     int accumulate;  // out += result instead of out = result
+    V4<R>* part_a;   // force partials (kernels with FORCE)
 };
 
 // Backward elementwise update of one step (applied to X after the VJP of the step before):
@@ -98,7 +105,10 @@ __device__ __forceinline__ R inv_sqrt(R x) {
 constexpr float kVjpPad = 1e18f;
 
 // MGRAD = false: the mass gradient is not wanted (w of the result is 0), 4 operations less.
-template <bool USOFT, bool UMASS, bool MGRAD>
+// FORCE: the same pass also sums the force a_k = sum_j m_j f d (3 operations more, 4 with
+// unequal masses) into p.part_a, and every result goes to the split partials (a finish pass
+// always follows).
+template <bool USOFT, bool UMASS, bool MGRAD, bool FORCE>
 __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float> p, float um) {
     __shared__ float4 s_xy[kBS];
     __shared__ float4 s_zm[kBS];
@@ -141,6 +151,7 @@ __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float
     }
     const float2 z2 = make_float2(0.f, 0.f);
     float2 Ax = z2, Ay = z2, Az = z2, Bx = z2, By = z2, Bz = z2, Mm = z2;
+    float2 Fx = z2, Fy = z2, Fz = z2;
 
     const int64_t jb = static_cast<int64_t>(blockIdx.y) * p.jchunk;
     const int64_t je = min(n, jb + p.jchunk);
@@ -173,6 +184,7 @@ __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float
             }
         }
         float2 tAx = z2, tAy = z2, tAz = z2, tBx = z2, tBy = z2, tBz = z2, tM = z2;
+        float2 tFx = z2, tFy = z2, tFz = z2;
 #pragma unroll 4
         for (int q = 0; q < kBS; ++q) {
             const float4 xy = s_xy[q], zm = s_zm[q], lxy = s_lxy[q], lzh = s_lzh[q];
@@ -213,6 +225,12 @@ __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float
                 const float2 dl = __ffma2_rn(dz, ljz, __ffma2_rn(dy, ljy, __fmul2_rn(dx, ljx)));
                 tM = __ffma2_rn(f, dl, tM);
             }
+            if constexpr (FORCE) {
+                const float2 fm = UMASS ? f : __fmul2_rn(make_float2(zm.z, zm.w), f);
+                tFx = __ffma2_rn(fm, dx, tFx);
+                tFy = __ffma2_rn(fm, dy, tFy);
+                tFz = __ffma2_rn(fm, dz, tFz);
+            }
         }
         Ax = __fadd2_rn(Ax, tAx);
         Ay = __fadd2_rn(Ay, tAy);
@@ -221,6 +239,11 @@ __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float
         By = __fadd2_rn(By, tBy);
         Bz = __fadd2_rn(Bz, tBz);
         Mm = __fadd2_rn(Mm, tM);
+        if constexpr (FORCE) {
+            Fx = __fadd2_rn(Fx, tFx);
+            Fy = __fadd2_rn(Fy, tFy);
+            Fz = __fadd2_rn(Fz, tFz);
+        }
     }
     const float sc = UMASS ? um : 1.f;
     const float gx[2] = {sc * (Ax.x - 3.f * Bx.x), sc * (Ax.y - 3.f * Bx.y)};
@@ -231,8 +254,13 @@ __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float
     for (int e = 0; e < 2; ++e) {
         const int64_t k = kbase + e * kBS + tid;
         if (k >= n) continue;
-        if (gridDim.y > 1) {
-            p.part[static_cast<int64_t>(blockIdx.y) * n + k] = v4<float>(gx[e], gy[e], gz[e], gm[e]);
+        if (FORCE || gridDim.y > 1) {
+            const int64_t o = static_cast<int64_t>(blockIdx.y) * n + k;
+            p.part[o] = v4<float>(gx[e], gy[e], gz[e], gm[e]);
+            if constexpr (FORCE) {
+                p.part_a[o] = e ? v4<float>(sc * Fx.y, sc * Fy.y, sc * Fz.y, 0.f)
+                                : v4<float>(sc * Fx.x, sc * Fy.x, sc * Fz.x, 0.f);
+            }
         } else if (p.accumulate) {
             const V4<float> o = p.out[k];
             p.out[k] = v4<float>(o.x + gx[e], o.y + gy[e], o.z + gz[e], o.w + gm[e]);
@@ -435,7 +463,7 @@ int vjp_f32x2_splits(int64_t n, int sms) {
     if (!resident) {
         int nb = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &nb, reinterpret_cast<const void*>(&vjp_f32x2_kernel<true, true, true>), kBS, 0) !=
+                &nb, reinterpret_cast<const void*>(&vjp_f32x2_kernel<true, true, true, false>), kBS, 0) !=
                 cudaSuccess ||
             nb < 1) {
             (void)cudaGetLastError();
@@ -485,10 +513,11 @@ void vjp_f32x2_launch(const void* posm, const void* hsoft, double uniform_h, dou
     p.out = static_cast<V4<float>*>(out);
     p.part = static_cast<V4<float>*>(part);
     p.accumulate = accumulate ? 1 : 0;
+    p.part_a = nullptr;
     RRG_REQUIRE(real == 1 || part != nullptr, RRG_ERR_STATE, "vjp: missing split partials");
     dim3 grid(static_cast<unsigned>((n + 2 * kBS - 1) / (2 * kBS)), real);
     const float um = uniform_m >= 0 ? static_cast<float>(uniform_m) : 1.f;
-#define RRG_VJP2(US, UM, MG) vjp_f32x2_kernel<US, UM, MG><<<grid, kBS, 0, stream>>>(p, um)
+#define RRG_VJP2(US, UM, MG) vjp_f32x2_kernel<US, UM, MG, false><<<grid, kBS, 0, stream>>>(p, um)
 #define RRG_VJP2_M(US, UM) \
     do {                   \
         if (mgrad)         \
@@ -512,6 +541,115 @@ void vjp_f32x2_launch(const void* posm, const void* hsoft, double uniform_h, dou
     } else if (upd.V) {
         adjoint_update_launch(n, out, upd, stream);
     }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Reverse leapfrog between checkpoints (FP32 backward). The step x' = x + dt v + dt^2/2 a(x),
+// v' = v + dt/2 (a(x) + a(x')) inverts exactly in real arithmetic:
+//   w = v' - dt/2 a(x'),  x = x' - dt w,  v = w - dt/2 a(x),
+// so the backward sweep rebuilds x_m from the state at m + 1, the force a(x_m) coming out of
+// the same pass over the pairs as the VJP at x_m. In FP32 each reversed step rounds once more
+// than the forward did, and every segment starts again from an exact checkpoint.
+struct RevStep {
+    const V4<float>* x;  // x_m (positions and masses)
+    V4<float>* x_next;   // x_{m-1} out, or nullptr
+    V4<float>* w;        // half-step velocity, updated in place: w -= dt a(x_m)
+    float dt;
+};
+
+// Top of a segment: w = v - dt/2 a, x_out = x - dt w (mass carried).
+__global__ void reverse_init_kernel(int64_t n, const V4<float>* __restrict__ x,
+                                    const V4<float>* __restrict__ v,
+                                    const V4<float>* __restrict__ a, V4<float>* __restrict__ w,
+                                    V4<float>* __restrict__ x_out, float dt) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float h = 0.5f * dt;
+    const V4<float> vi = v[i], ai = a[i], xi = x[i];
+    const V4<float> wi = v4<float>(vi.x - h * ai.x, vi.y - h * ai.y, vi.z - h * ai.z, 0.f);
+    w[i] = wi;
+    x_out[i] = v4<float>(xi.x - dt * wi.x, xi.y - dt * wi.y, xi.z - dt * wi.z, xi.w);
+}
+
+// Finish of a FORCE pass at x_m: X += sum of the VJP partials (fixed order, FP64), a(x_m) from
+// the force partials, w -= dt a, x_{m-1} = x_m - dt w, then the adjoint update of step m - 1.
+__global__ void vjp_reverse_finish(const VjpParams<float> p, int splits, const AdjUpd<float> upd,
+                                   const RevStep r) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= p.n) return;
+    double sx = 0, sy = 0, sz = 0, sm = 0, ax = 0, ay = 0, az = 0;
+    for (int s = 0; s < splits; ++s) {
+        const int64_t o = static_cast<int64_t>(s) * p.n + k;
+        const V4<float> v = p.part[o];
+        sx += v.x;
+        sy += v.y;
+        sz += v.z;
+        sm += v.w;
+        const V4<float> a = p.part_a[o];
+        ax += a.x;
+        ay += a.y;
+        az += a.z;
+    }
+    const V4<float> o = p.out[k];
+    const V4<float> X = v4<float>(static_cast<float>(sx + o.x), static_cast<float>(sy + o.y),
+                                  static_cast<float>(sz + o.z), static_cast<float>(sm + o.w));
+    p.out[k] = X;
+    V4<float> w = r.w[k];
+    w.x -= r.dt * static_cast<float>(ax);
+    w.y -= r.dt * static_cast<float>(ay);
+    w.z -= r.dt * static_cast<float>(az);
+    r.w[k] = w;
+    if (r.x_next) {
+        const V4<float> x = r.x[k];
+        r.x_next[k] = v4<float>(x.x - r.dt * w.x, x.y - r.dt * w.y, x.z - r.dt * w.z, x.w);
+    }
+    if (upd.V) adjoint_update_at(k, X.x, X.y, X.z, upd);
+}
+
+// One reverse step at x_m = r.x: VJP with cotangent lam accumulated into out (= X), a(x_m),
+// the reverse update of (w, positions) and the adjoint update upd. part / part_a hold
+// [splits][n] V4 each.
+void vjp_reverse_launch(const void* hsoft, double uniform_h, double uniform_m, int64_t n,
+                        const void* lam, void* out, void* part, void* part_a, int splits,
+                        cudaStream_t stream, const AdjUpd<float>& upd, const RevStep& r,
+                        bool mgrad) {
+    const int64_t tiles = (n + kBS - 1) / kBS;
+    const int64_t tiles_per = (tiles + splits - 1) / splits;
+    const int real = static_cast<int>((tiles + tiles_per - 1) / tiles_per);
+    RRG_REQUIRE(part && part_a, RRG_ERR_STATE, "vjp: missing partials");
+    VjpParams<float> p;
+    p.posm = r.x;
+    p.hsoft = static_cast<const float*>(hsoft);
+    p.uniform_h = static_cast<float>(uniform_h);
+    p.n = n;
+    p.jchunk = tiles_per * kBS;
+    p.lam = static_cast<const V4<float>*>(lam);
+    p.out = static_cast<V4<float>*>(out);
+    p.part = static_cast<V4<float>*>(part);
+    p.accumulate = 1;
+    p.part_a = static_cast<V4<float>*>(part_a);
+    dim3 grid(static_cast<unsigned>((n + 2 * kBS - 1) / (2 * kBS)), real);
+    const float um = uniform_m >= 0 ? static_cast<float>(uniform_m) : 1.f;
+#define RRG_VJPF(US, UM, MG) vjp_f32x2_kernel<US, UM, MG, true><<<grid, kBS, 0, stream>>>(p, um)
+#define RRG_VJPF_M(US, UM)          \
+    do {                            \
+        if (mgrad)                  \
+            RRG_VJPF(US, UM, true); \
+        else                        \
+            RRG_VJPF(US, UM, false); \
+    } while (0)
+    if (uniform_m >= 0) {
+        if (hsoft) RRG_VJPF_M(false, true);
+        else RRG_VJPF_M(true, true);
+    } else {
+        if (hsoft) RRG_VJPF_M(false, false);
+        else RRG_VJPF_M(true, false);
+    }
+#undef RRG_VJPF_M
+#undef RRG_VJPF
+    RRG_LAUNCHED();
+    vjp_reverse_finish<<<div_up(n, 256), 256, 0, stream>>>(p, real, upd, r);
+    RRG_LAUNCHED();
 }
 
 // Does every particle's mass equal posm[0].w?  flags[0] (zeroed by the caller) becomes 1 on a
@@ -620,6 +758,8 @@ struct rrg_adjoint {
     ABuf seg_x;            // (every + 1) x n x V4
     ABuf x, x2, v, a, u, X, V, c, g, xN, scratch, sym_slots;
     ABuf vjp_part;          // FP32: j-split partials of the paired VJP
+    ABuf vjp_part_a;        // FP32: force partials of the reverse steps
+    ABuf w;                 // FP32: half-step velocity of the reverse steps
     ABuf mflags;            // uniform-mass check: mismatch flag, mass bits
     int splits = 1;
     int vjp_splits = 1;
@@ -808,7 +948,7 @@ RRG_API rrg_status rrg_adjoint_create(int device, int precision, int64_t n, doub
         A->ckpt_x.alloc(vb(A) * nck);
         A->ckpt_v.alloc(vb(A) * nck);
         A->ckpt_a.alloc(vb(A) * nck);
-        A->seg_x.alloc(vb(A) * (A->every + 1));
+        if (precision == RRG_PREC_FP64) A->seg_x.alloc(vb(A) * (A->every + 1));
         for (ABuf* b : {&A->x, &A->x2, &A->v, &A->a, &A->u, &A->X, &A->V, &A->c, &A->g, &A->xN})
             b->alloc(vb(A));
         const int sms = num_sms(device);
@@ -819,8 +959,12 @@ RRG_API rrg_status rrg_adjoint_create(int device, int precision, int64_t n, doub
             A->sym_slots.alloc(vjp_sym_slot_bytes<double>(n));
         } else {
             A->vjp_splits = vjp_f32x2_splits(n, sms);
-            const size_t pb = vjp_f32x2_part_bytes(n, A->vjp_splits);
-            if (pb) A->vjp_part.alloc(pb);
+            // the reverse steps write partials even with one split
+            const size_t pb = sizeof(V4<float>) * static_cast<size_t>(n) *
+                              static_cast<size_t>(std::max(1, A->vjp_splits));
+            A->vjp_part.alloc(pb);
+            A->vjp_part_a.alloc(pb);
+            A->w.alloc(vb(A));
         }
         A->mflags.alloc(16);
         *out = A;
@@ -916,10 +1060,42 @@ RRG_API rrg_status rrg_adjoint_backward(rrg_adjoint* A, const void* gx_final,
             RRG_LAUNCHED();
         }
         const int nseg = (A->nsteps + A->every - 1) / A->every;
-        for (int seg = nseg - 1; seg >= 0; --seg) {
+        for (int seg = nseg - 1; seg >= 0 && A->prec == RRG_PREC_FP32; --seg) {
+            // FP32: reverse steps from the state at the segment's top (the next checkpoint, or
+            // the final state) down to n0 + 1, each one pass of the fused VJP + force kernel;
+            // x_n0 is the checkpoint itself
             const int n0 = seg * A->every;
             const int n1 = std::min(A->nsteps, n0 + A->every);
-            // recompute the segment from its checkpoint: x_n0 is the checkpoint itself, x_n for
+            char* xc = A->ckpt_x.c() + b * seg;
+            if (n1 - n0 > 1) {
+                const bool last = seg == nseg - 1;
+                const size_t top = static_cast<size_t>(seg + 1);
+                const void* xt = last ? A->xN.p : A->ckpt_x.c() + b * top;
+                const void* vt = last ? A->v.p : A->ckpt_v.c() + b * top;
+                const void* at = last ? A->a.p : A->ckpt_a.c() + b * top;
+                char* xbuf[2] = {A->x.c(), A->x2.c()};
+                reverse_init_kernel<<<div_up(A->n, 256), 256, 0, s>>>(
+                    A->n, static_cast<const V4<float>*>(xt), static_cast<const V4<float>*>(vt),
+                    static_cast<const V4<float>*>(at), static_cast<V4<float>*>(A->w.p),
+                    reinterpret_cast<V4<float>*>(xbuf[(n1 - 1) & 1]), static_cast<float>(A->dt));
+                RRG_LAUNCHED();
+                for (int m = n1 - 1; m > n0; --m) {
+                    RevStep r;
+                    r.x = reinterpret_cast<const V4<float>*>(xbuf[m & 1]);
+                    r.x_next = m - 1 > n0 ? reinterpret_cast<V4<float>*>(xbuf[(m - 1) & 1]) : nullptr;
+                    r.w = static_cast<V4<float>*>(A->w.p);
+                    r.dt = static_cast<float>(A->dt);
+                    vjp_reverse_launch(A->hsoft.p, A->uniform_h, A->uniform_m, A->n, A->c.p, A->X.p,
+                                       A->vjp_part.p, A->vjp_part_a.p, A->vjp_splits, s,
+                                       step_update<float>(A, m - 1), r, A->mass_grad);
+                }
+            }
+            vjp(A, xc, n0 - 1, s);
+        }
+        for (int seg = nseg - 1; seg >= 0 && A->prec == RRG_PREC_FP64; --seg) {
+            const int n0 = seg * A->every;
+            const int n1 = std::min(A->nsteps, n0 + A->every);
+            // FP64: recompute the segment from its checkpoint: x_n0 is the checkpoint itself, x_n for
             // n0 < n < n1 go to seg_x[n - n0] (a predict, then fused steps)
             char* xc = A->ckpt_x.c() + b * seg;
             if (n1 - n0 > 1) {

@@ -137,6 +137,8 @@ def lib() -> C.CDLL:
         "rrg_project_grid_acceleration_on_particles": (st, [vp]),
         "rrg_project_grid_grav_on_particles": (st, [vp]),
         "rrg_calc_conservation": (st, [vp, C.POINTER(Conservation)]),
+        "rrg_calc_conservation_async": (st, [vp, vp]),
+        "rrg_conservation_from_sums": (st, [vp, C.c_double, C.POINTER(Conservation)]),
         "rrg_calc_mass_center": (st, [vp, d, d]),
         "rrg_solver_init": (st, [vp, C.POINTER(SimParams)]),
         "rrg_solver_precalc": (st, [vp]),
@@ -325,6 +327,13 @@ class Context:
         self._c(lib().rrg_calc_conservation(self._h, C.byref(c)))
         return c.as_dict()
 
+    def calc_conservation_async(self, sums: np.ndarray) -> None:
+        """Enqueue the conservation sums into `sums` (12 float64, ideally pinned); no wait.
+        Read them once the context stream has passed this point (conservation_from_sums)."""
+        if sums.dtype != np.float64 or sums.size < 12 or not sums.flags["C_CONTIGUOUS"]:
+            raise RRGError(1, "calc_conservation_async: needs 12 contiguous float64")
+        self._c(lib().rrg_calc_conservation_async(self._h, sums.ctypes.data))
+
     def calc_mass_center(self):
         com = np.empty(3)
         m = C.c_double()
@@ -440,6 +449,14 @@ def make_ensemble(ngal: int = 64, nmin: int = 1024, nmax: int = 65536, seed: int
 
 
 # -- host I/O --------------------------------------------------------------------------------
+def conservation_from_sums(sums: np.ndarray, time: float = 0.0) -> dict:
+    """Ek, Ep, momentum and angular momentum from the 12 sums of calc_conservation_async."""
+    s = np.ascontiguousarray(sums, dtype=np.float64)
+    c = Conservation()
+    check(lib().rrg_conservation_from_sums(s.ctypes.data, float(time), C.byref(c)))
+    return c.as_dict()
+
+
 def parse_params_json(path) -> ParsedParams:
     p = ParsedParams()
     check(lib().rrg_parse_params_json(str(path).encode(), C.byref(p)))

@@ -132,10 +132,15 @@ struct rrg_ctx {
     double time = 0.0;
     uint64_t iter = 0;
     int sort_interval = -1;          // -1: the strategy's default (64 steps in wave mode)
+    // Wave mode, between calc_steps calls: the last particle pass also predicted the next step,
+    // so posm[1 - cur] (and poslo[1 - cur]) hold x_{n+1}, u its v + v*, and mg[1 - mg_cur] its
+    // deposit. The synced state (x_n, v_n, a_n, deposit of x_n) is untouched; the next
+    // calc_steps adopts the prediction instead of predicting again.
+    bool pending = false;
     int64_t steps_since_sort = INT64_MAX / 2;
     Buf sort_keys, sort_dest, sort_counts, sort_offsets, sort_cursor, sort_temp, sort_stage;
     size_t sort_temp_bytes = 0;
-    std::map<std::tuple<int, int, int, int>, GraphExec> graphs;
+    std::map<std::tuple<int, int, int, int, bool>, GraphExec> graphs;
 
     ~rrg_ctx() {
         for (auto& kv : graphs)
@@ -328,6 +333,14 @@ void deposit_operator(rrg_ctx* c) {
     c->src_dirty = true;
 }
 
+// Discards a pending prediction (any call that changes the state); clears its deposit so that
+// mg[1 - mg_cur] is zero again.
+void drop_pending(rrg_ctx* c) {
+    if (!c->pending) return;
+    RRG_CUDA(cudaMemsetAsync(c->mg[1 - c->mg_cur].p, 0, c->mg[1 - c->mg_cur].bytes, c->stream));
+    c->pending = false;
+}
+
 // Counting sort of the synced particle state by CIC base cell. Every array is scattered into a
 // staging buffer and copied back in place, so buffer addresses (and recorded graphs) stay.
 void sort_particles(rrg_ctx* c) {
@@ -404,9 +417,12 @@ void record_nbody_steps(rrg_ctx* c, int nsteps) {
 
 // Wave: [predict + deposit] then per step: source, `iterations` substeps, gradient, fused
 // particle pass (interp + correct [+ next predict + deposit]).
-void record_wave_steps(rrg_ctx* c, int nsteps) {
+// prologue = false: the chunk starts from an adopted prediction (see rrg_ctx::pending). The
+// last pass corrects and syncs step n and already predicts step n + 1 into the other position
+// buffer and the zeroed deposit grid, leaving the synced state in place.
+void record_wave_steps(rrg_ctx* c, int nsteps, bool prologue) {
     const WaveCoef w = wave_coef(c);
-    {
+    if (prologue) {
         const int t = 1 - c->mg_cur;  // known zero
         PmParticleArgs a = pm_args(c, t);
         launch_pm_particles(a, PM_PREDICT_DEPOSIT, c->stream);
@@ -422,8 +438,11 @@ void record_wave_steps(rrg_ctx* c, int nsteps) {
             launch_pm_particles(a, PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT, c->stream);
             c->mg_cur = t;
         } else {
-            PmParticleArgs a = pm_args(c, -1);
-            launch_pm_particles(a, PM_INTERP_CORRECT | PM_WRITE_SYNC, c->stream);
+            PmParticleArgs a = pm_args(c, 1 - c->mg_cur);  // zeroed by this step's source pass
+            a.pos_out = c->posm[1 - c->cur].p;
+            a.lo_out = c->prec == RRG_PREC_MIXED ? c->poslo[1 - c->cur].p : nullptr;
+            launch_pm_particles(a, PM_INTERP_CORRECT | PM_WRITE_SYNC | PM_PREDICT_DEPOSIT,
+                                c->stream);
         }
     }
 }
@@ -443,7 +462,15 @@ void wave_steps_unfused(rrg_ctx* c, int nsteps) {
 }
 
 void run_graph(rrg_ctx* c, int nsteps) {
-    const auto key = std::make_tuple(nsteps, c->cur, c->mg_cur, c->phi_cur);
+    bool prologue = true;
+    if (c->wave_mode && c->pending) {
+        // adopt the prediction the previous chunk left
+        c->cur = 1 - c->cur;
+        c->mg_cur = 1 - c->mg_cur;
+        c->pending = false;
+        prologue = false;
+    }
+    const auto key = std::make_tuple(nsteps, c->cur, c->mg_cur, c->phi_cur, prologue);
     auto it = c->graphs.find(key);
     const int cur0 = c->cur, mg0 = c->mg_cur, phi0 = c->phi_cur;
     if (it == c->graphs.end()) {
@@ -451,7 +478,7 @@ void run_graph(rrg_ctx* c, int nsteps) {
         RRG_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         set_capturing(true);
         try {
-            if (c->wave_mode) record_wave_steps(c, nsteps);
+            if (c->wave_mode) record_wave_steps(c, nsteps, prologue);
             else record_nbody_steps(c, nsteps);
         } catch (...) {
             set_capturing(false);
@@ -481,7 +508,8 @@ void run_graph(rrg_ctx* c, int nsteps) {
     } else {
         // replaying: advance the buffer roles exactly as recording did
         if (c->wave_mode) {
-            c->mg_cur = (nsteps % 2 == 1) ? 1 - mg0 : mg0;
+            const int flips = prologue ? nsteps : nsteps - 1;
+            c->mg_cur = (flips % 2 == 1) ? 1 - mg0 : mg0;
             if (c->wave.iterations % 2 == 1) c->phi_cur = (nsteps % 2 == 1) ? 1 - phi0 : phi0;
         } else {
             c->cur = ((nsteps - 1) % 2 == 1) ? 1 - cur0 : cur0;
@@ -489,6 +517,7 @@ void run_graph(rrg_ctx* c, int nsteps) {
     }
     RRG_CUDA(cudaGraphLaunch(it->second.exec, c->stream));
     count_launches(it->second.kernels);
+    if (c->wave_mode) c->pending = true;
 }
 
 }  // namespace
@@ -563,6 +592,7 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
                                       const double* vel, const double* mass,
                                       const double* soft2) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         RRG_REQUIRE(n >= 1, RRG_ERR_INVALID, "rrg_load_particles: n must be >= 1");
         RRG_REQUIRE(n < (int64_t(1) << 31), RRG_ERR_INVALID,
                     "rrg_load_particles: n must be < 2^31");
@@ -696,6 +726,7 @@ RRG_API rrg_status rrg_get_time(const rrg_ctx* ctx, double* time, uint64_t* iter
 
 RRG_API rrg_status rrg_init_grid(rrg_ctx* ctx, const rrg_grid_info* grid) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         RRG_REQUIRE(grid != nullptr, RRG_ERR_INVALID, "rrg_init_grid: NULL grid");
         RRG_REQUIRE(grid->nx >= 2 && grid->nx <= 1024, RRG_ERR_INVALID,
                     "rrg_init_grid: nx must be in [2, 1024]");
@@ -732,6 +763,7 @@ RRG_API rrg_status rrg_init_grid(rrg_ctx* ctx, const rrg_grid_info* grid) {
 
 RRG_API rrg_status rrg_set_wave_params(rrg_ctx* ctx, const rrg_wave_params* wave) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         RRG_REQUIRE(wave != nullptr, RRG_ERR_INVALID, "rrg_set_wave_params: NULL");
         RRG_REQUIRE(std::isfinite(wave->dt) && wave->dt > 0, RRG_ERR_INVALID,
                     "rrg_set_wave_params: dt must be positive (0.5 dx / (c sqrt 3))");
@@ -789,6 +821,7 @@ RRG_API rrg_status rrg_get_grid(rrg_ctx* ctx, double* mass, double* grav, double
 
 RRG_API rrg_status rrg_set_grid_potential(rrg_ctx* ctx, const double* grav) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_grid(ctx);
         RRG_REQUIRE(grav != nullptr, RRG_ERR_INVALID, "rrg_set_grid_potential: NULL");
         const size_t nc = static_cast<size_t>(ctx->grid.nx) * ctx->grid.nx * ctx->grid.nx;
@@ -813,6 +846,7 @@ RRG_API rrg_status rrg_get_deposit_scale(const rrg_ctx* ctx, int32_t* shift_s) {
 // ---------------------------------------------------------------------------------------------
 RRG_API rrg_status rrg_predict_step(rrg_ctx* ctx, double dt) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_particles(ctx);
         launch_predict(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->acc.p, ctx->u.p,
                        dt, ctx->stream);
@@ -821,6 +855,7 @@ RRG_API rrg_status rrg_predict_step(rrg_ctx* ctx, double dt) {
 
 RRG_API rrg_status rrg_nbody_acceleration(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_particles(ctx);
         DirectEpi e;
         e.mode = EPI_STORE;
@@ -844,6 +879,7 @@ RRG_API rrg_status rrg_nbody_grav(rrg_ctx* ctx) {
 
 RRG_API rrg_status rrg_correct_step(rrg_ctx* ctx, double dt) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_particles(ctx);
         launch_correct(ctx->prec, ctx->n, ctx->vel.p, ctx->acc.p, ctx->u.p, dt, ctx->stream);
     })
@@ -851,6 +887,7 @@ RRG_API rrg_status rrg_correct_step(rrg_ctx* ctx, double dt) {
 
 RRG_API rrg_status rrg_convert_particles_to_grid(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_particles(ctx);
         require_grid(ctx);
         deposit_operator(ctx);
@@ -859,6 +896,7 @@ RRG_API rrg_status rrg_convert_particles_to_grid(rrg_ctx* ctx) {
 
 RRG_API rrg_status rrg_set_boundary_periodic(rrg_ctx* ctx, double total_mass, int keep_layer) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_grid(ctx);
         set_periodic(ctx, total_mass, keep_layer);
     })
@@ -867,6 +905,7 @@ RRG_API rrg_status rrg_set_boundary_periodic(rrg_ctx* ctx, double total_mass, in
 RRG_API rrg_status rrg_set_boundary_monopole(rrg_ctx* ctx, double total_mass,
                                              const double center_of_mass[3], int radiative) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_grid(ctx);
         RRG_REQUIRE(center_of_mass != nullptr, RRG_ERR_INVALID, "NULL centre of mass");
         drop_graphs(ctx);
@@ -882,6 +921,7 @@ RRG_API rrg_status rrg_set_boundary_monopole(rrg_ctx* ctx, double total_mass,
 
 RRG_API rrg_status rrg_set_boundary_zero(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_grid(ctx);
         drop_graphs(ctx);
         ctx->bc_type = RRG_BC_ZERO_DIRICHLET;
@@ -893,6 +933,7 @@ RRG_API rrg_status rrg_set_boundary_zero(rrg_ctx* ctx) {
 RRG_API rrg_status rrg_solve_wave_equation(rrg_ctx* ctx, int max_iterations,
                                            int* iterations_run, double* last_rel_diff) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         const int it = solve_wave(ctx, max_iterations, last_rel_diff);
         if (iterations_run) *iterations_run = it;
     })
@@ -900,6 +941,7 @@ RRG_API rrg_status rrg_solve_wave_equation(rrg_ctx* ctx, int max_iterations,
 
 RRG_API rrg_status rrg_calc_acceleration_field(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_grid(ctx);
         gradient(ctx);
     })
@@ -907,6 +949,7 @@ RRG_API rrg_status rrg_calc_acceleration_field(rrg_ctx* ctx) {
 
 RRG_API rrg_status rrg_project_grid_acceleration_on_particles(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_particles(ctx);
         require_grid(ctx);
         launch_interp(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->gdev, ctx->acc4.p, ctx->acc.p,
@@ -949,6 +992,32 @@ RRG_API rrg_status rrg_calc_conservation(rrg_ctx* ctx, rrg_conservation* out) {
     })
 }
 
+RRG_API rrg_status rrg_calc_conservation_async(rrg_ctx* ctx, double* sums) {
+    RRG_ENTRY(ctx, {
+        require_particles(ctx);
+        RRG_REQUIRE(sums != nullptr, RRG_ERR_INVALID, "NULL output");
+        const int rb = conservation_blocks(ctx->n);
+        launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
+                            ctx->red_partial.as<double>(), rb, ctx->red_out.as<double>(),
+                            ctx->stream);
+        RRG_CUDA(cudaMemcpyAsync(sums, ctx->red_out.p, 12 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    })
+}
+
+RRG_API rrg_status rrg_conservation_from_sums(const double* sums, double time,
+                                              rrg_conservation* out) {
+    if (!sums || !out) return RRG_ERR_INVALID;
+    out->time = time;
+    out->Ek = 0.5 * sums[0];
+    out->Ep = 0.5 * sums[1];
+    for (int k = 0; k < 3; ++k) {
+        out->momentum[k] = sums[2 + k];
+        out->angular[k] = sums[5 + k];
+    }
+    return RRG_OK;
+}
+
 RRG_API rrg_status rrg_calc_mass_center(rrg_ctx* ctx, double center_of_mass[3],
                                         double* total_mass) {
     RRG_ENTRY(ctx, {
@@ -965,6 +1034,7 @@ RRG_API rrg_status rrg_calc_mass_center(rrg_ctx* ctx, double center_of_mass[3],
 // ---------------------------------------------------------------------------------------------
 RRG_API rrg_status rrg_solver_init(rrg_ctx* ctx, const rrg_sim_params* sim) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         require_particles(ctx);
         RRG_REQUIRE(sim != nullptr, RRG_ERR_INVALID, "NULL sim params");
         RRG_REQUIRE(std::isfinite(sim->dt_dynamics) && sim->dt_dynamics > 0, RRG_ERR_INVALID,
@@ -986,6 +1056,7 @@ RRG_API rrg_status rrg_solver_init(rrg_ctx* ctx, const rrg_sim_params* sim) {
 
 RRG_API rrg_status rrg_solver_precalc(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
+        drop_pending(ctx);
         RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
         if (ctx->wave_mode) {
             deposit_operator(ctx);
@@ -1012,9 +1083,10 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
                 ctx->wave_mode && ctx->wave.steady_check_step > 0 &&
                 ctx->wave.iterations > ctx->wave.steady_check_step;
             if (checks_inside) {
+                drop_pending(ctx);
                 wave_steps_unfused(ctx, nsteps);
             } else {
-                if (ctx->wave_mode && ctx->src_dirty) {
+                if (ctx->wave_mode && ctx->src_dirty && !ctx->pending) {
                     // keep the invariant "mg[1 - mg_cur] is zero" before the fused steps
                     RRG_CUDA(cudaMemsetAsync(ctx->mg[1 - ctx->mg_cur].p, 0,
                                              ctx->mg[1 - ctx->mg_cur].bytes, ctx->stream));
@@ -1027,7 +1099,10 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
                 while (left > 0) {
                     int chunk = std::min(left, 64);
                     if (interval > 0) {
-                        if (ctx->steps_since_sort >= interval) sort_particles(ctx);
+                        if (ctx->steps_since_sort >= interval) {
+                            drop_pending(ctx);  // the sort permutes the synced state only
+                            sort_particles(ctx);
+                        }
                         chunk = static_cast<int>(
                             std::min<int64_t>(chunk, interval - ctx->steps_since_sort));
                     }

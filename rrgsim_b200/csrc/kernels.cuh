@@ -138,6 +138,8 @@ struct PmParticleArgs {
     int shift_s;
     unsigned long long* mgrid;
     double dt;
+    void* pos_out = nullptr;  // predicted positions (and MIXED low parts) go here when set,
+    void* lo_out = nullptr;   // else they overwrite posm / poslo in place
 };
 void launch_pm_particles(const PmParticleArgs& a, int mode, cudaStream_t s);
 

@@ -171,6 +171,23 @@ def test_conservation_reductions(prec):
     assert abs(mt - rm) <= 1e-12
 
 
+def test_asynchronous_conservation_sums_equal_the_synchronous_ones():
+    n = 3000
+    pos, vel, m, s2 = plummer(n, seed=8)
+    sums = np.full((3, 12), np.nan)
+    with _ctx("fp32", pos, vel, m, s2) as c:
+        c.nbody_grav()
+        ref = c.calc_conservation()
+        for k in range(3):  # several in flight, the stream orders them
+            c.calc_conservation_async(sums[k])
+        c.synchronize()
+    for k in range(3):
+        got = rg.conservation_from_sums(sums[k])
+        assert got["Ek"] == ref["Ek"] and got["Ep"] == ref["Ep"]
+        np.testing.assert_array_equal(got["momentum"], ref["momentum"])
+        np.testing.assert_array_equal(got["angular"], ref["angular"])
+
+
 def test_raw_device_entry_points_match_context():
     torch = pytest.importorskip("torch")
     n = 3000

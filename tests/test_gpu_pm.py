@@ -280,3 +280,53 @@ def test_nbody_sync_projects_particles_on_grid(prec):
     occupied = np.bincount(orc.ngp_cell(held_pos, og), minlength=nx ** 3) > 0
     assert np.all(grid["grav"][~occupied] == 0.0)
     assert np.all(grid["grav"][occupied] < 0.0)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("interval", [0, 4])
+def test_step_by_step_calls_equal_one_long_call(prec, interval):
+    """Each calc_steps call ends by predicting the next step (kept pending, adopted by the next
+    call); reads in between see the synced state. One call of 12 steps, 12 calls of one step
+    and calls split around reads give the same bits."""
+    nx, n, dt = 32, 20000, 2e-3
+    pos, vel, m, s2 = disk(n, seed=5)
+    g = _grid(nx)
+    vmax = np.max(np.linalg.norm(vel, axis=1))
+    wp = rg.WaveParams.make(g.dx, diss_base=1.0 / (4 * g.dx), wave_speed=10 * vmax,
+                            iterations=20, setup_iterations=200, steady_check_step=1000)
+    sim = rg.SimParams(time_max=1.0, dt_save=0.1, dt_dynamics=dt, saves_without_dump=2 ** 63,
+                       use_wave_model=1)
+    out = []
+    for plan in ("long", "single", "split"):
+        with _ctx(prec, pos, vel, m, s2, g) as c:
+            c.set_sort_interval(interval)
+            c.set_wave_params(wp)
+            c.solver_init(sim)
+            c.precalc()
+            if plan == "long":
+                c.calc_steps(12)
+            elif plan == "single":
+                for _ in range(12):
+                    c.calc_steps(1)
+            else:
+                c.calc_steps(5)
+                mid = c.get_particles()
+                c.calc_conservation()
+                c.get_grid()
+                c.calc_steps(7)
+            out.append((c.get_particles(), c.get_grid()))
+            if plan == "split":
+                with _ctx(prec, pos, vel, m, s2, g) as r:
+                    r.set_sort_interval(interval)
+                    r.set_wave_params(wp)
+                    r.solver_init(sim)
+                    r.precalc()
+                    r.calc_steps(5)
+                    ref_mid = r.get_particles()
+                for k in ("pos", "vel", "acc"):
+                    np.testing.assert_array_equal(mid[k], ref_mid[k])
+    for p, gr in out[1:]:
+        for k in ("pos", "vel", "acc"):
+            np.testing.assert_array_equal(p[k], out[0][0][k])
+        np.testing.assert_array_equal(gr["mass"], out[0][1]["mass"])
+        np.testing.assert_array_equal(gr["grav"], out[0][1]["grav"])

@@ -281,7 +281,7 @@ def run_native(args):
     traffic = None
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("wave_periodic_kernel_bytes_per_launch")
+        traffic = json.loads(tf.read_text()).get("wave_periodic_x4_kernel_bytes_per_launch")
 
     # ---- end to end through the public API with host buffers ----------------------------------
     # the same run length as the device-timed region: ICs up once, K steps each followed by a
@@ -376,7 +376,7 @@ def run_native(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": k_e2e},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "wave_periodic_kernel", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "wave_periodic_x4_kernel", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_kind": how,
                          "ms_per_launch": wave_ms, "alg_bytes_per_launch": alg_bytes},

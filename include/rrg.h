@@ -275,6 +275,16 @@ RRG_API rrg_status rrg_solver_precalc(rrg_ctx* ctx);
 RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps);
 /* sync_particles_and_grid: potential (and, in wave mode, acceleration) on particles. */
 RRG_API rrg_status rrg_solver_sync(rrg_ctx* ctx);
+/* Precalc for a restored state (resume from a dump, wiring read_particles_dump,
+ * io_particles_bin.cu:39-77, which the reference never calls): N-body as precalc; wave mode
+ * deposits and takes the gradient of the potential set by rrg_set_wave_state, without the
+ * setup relaxation. */
+RRG_API rrg_status rrg_solver_resume(rrg_ctx* ctx);
+/* The two wave levels (current and previous, nx^3 FP64 each, x fastest) out of / into the
+ * context, for saving and restoring the wave state with a dump. */
+RRG_API rrg_status rrg_get_wave_state(rrg_ctx* ctx, double* phi_cur, double* phi_prev);
+RRG_API rrg_status rrg_set_wave_state(rrg_ctx* ctx, const double* phi_cur,
+                                      const double* phi_prev);
 
 /* Sorts particles by grid cell (counting sort) so deposits from one warp hit few cells.
  * Host-visible order is unchanged (rrg_get_particles undoes the permutation). The wave
@@ -312,11 +322,26 @@ RRG_API rrg_status rrg_write_dump(const char* dump_dir, uint64_t iter, double ti
 RRG_API rrg_status rrg_read_dump(const char* path, int64_t capacity, int64_t* n, double* time,
                                  double* pos, double* vel);
 
+/* The wave state beside a snapshot: <dir>/W_{iter:>5d}.bin = uint64 nx, float64 t,
+ * float64 phi_cur[nx^3], float64 phi_prev[nx^3]. No counterpart in the reference (its dump holds
+ * particles only); with it a wave-mode run resumes exactly. */
+RRG_API rrg_status rrg_write_wave_state(const char* dump_dir, uint64_t iter, double time,
+                                        int32_t nx, const double* phi_cur,
+                                        const double* phi_prev);
+RRG_API rrg_status rrg_read_wave_state(const char* path, int32_t nx, double* time,
+                                       double* phi_cur, double* phi_prev);
+
 /* The whole `rrgsim <work_dir>` run (solver/app/src/rrgsim.cu:12-62 and integrate(),
  * solver/app/src/rrgsim_integration.cu:19-146): parses params.json, reads the ICs (paths
  * relative to work_dir, '\' accepted), integrates on `device`, writes dump/ and data/.
  * Returns RRG_OK, or an error (the reference logs and exits 0). */
 RRG_API rrg_status rrg_run(const char* work_dir, int device, int precision);
+/* The same run continued from <work_dir>/dump/S_{iter:>5d}.bin (and W_{iter:>5d}.bin in wave
+ * mode) of an earlier run with the same params.json: masses and softening from the ICs,
+ * positions, velocities and time from the dump, the save cadence and dump count replayed up
+ * to that time, data/ tables appended to. `rrgsim <work_dir> --resume <iter>`. */
+RRG_API rrg_status rrg_run_resume(const char* work_dir, uint64_t iteration, int device,
+                                  int precision);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Synthetic initial conditions (no counterpart in the reference, which ships no generator)   */

@@ -144,6 +144,9 @@ def lib() -> C.CDLL:
         "rrg_solver_precalc": (st, [vp]),
         "rrg_solver_calc_steps": (st, [vp, i32]),
         "rrg_solver_sync": (st, [vp]),
+        "rrg_solver_resume": (st, [vp]),
+        "rrg_get_wave_state": (st, [vp, d, d]),
+        "rrg_set_wave_state": (st, [vp, d, d]),
         "rrg_set_sort_interval": (st, [vp, i32]),
         "rrg_parse_params_json": (st, [C.c_char_p, C.POINTER(ParsedParams)]),
         "rrg_read_ic_component": (st, [C.c_char_p, C.c_double, C.c_double, i64, i64, d, d, d, d,
@@ -153,6 +156,9 @@ def lib() -> C.CDLL:
         "rrg_write_dump": (st, [C.c_char_p, C.c_uint64, C.c_double, i64, d, d]),
         "rrg_read_dump": (st, [C.c_char_p, i64, C.POINTER(i64), d, d, d]),
         "rrg_run": (st, [C.c_char_p, i32, i32]),
+        "rrg_run_resume": (st, [C.c_char_p, C.c_uint64, i32, i32]),
+        "rrg_write_wave_state": (st, [C.c_char_p, C.c_uint64, C.c_double, i32, d, d]),
+        "rrg_read_wave_state": (st, [C.c_char_p, i32, d, d, d]),
         "rrg_generate_plummer": (st, [C.c_uint64, i64, C.c_double, C.c_double, C.c_double, d, d]),
         "rrg_generate_exp_disk": (st, [C.c_uint64, i64, C.c_double, C.c_double, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_double,
@@ -353,6 +359,21 @@ class Context:
     def sync_particles_and_grid(self) -> None:
         self._c(lib().rrg_solver_sync(self._h))
 
+    def resume(self) -> None:
+        """Precalc for a restored state: forces from the loaded positions and, in wave mode,
+        the potential set by set_wave_state (no setup relaxation)."""
+        self._c(lib().rrg_solver_resume(self._h))
+
+    def get_wave_state(self):
+        nc = self.grid.nx ** 3
+        cur, prev = np.empty(nc), np.empty(nc)
+        self._c(lib().rrg_get_wave_state(self._h, _d(cur), _d(prev)))
+        return cur, prev
+
+    def set_wave_state(self, cur, prev) -> None:
+        cur, prev = _f64(cur), _f64(prev)
+        self._c(lib().rrg_set_wave_state(self._h, _d(cur), _d(prev)))
+
     def set_sort_interval(self, interval: int) -> None:
         self._c(lib().rrg_set_sort_interval(self._h, int(interval)))
 
@@ -498,8 +519,20 @@ def read_dump(path):
     return t.value, pos, vel
 
 
-def run(work_dir, device: int = 0, precision: str = "fp32") -> None:
-    check(lib().rrg_run(str(work_dir).encode(), int(device), PREC[precision]))
+def run(work_dir, device: int = 0, precision: str = "fp32", resume: int | None = None) -> None:
+    """The rrgsim run of work_dir; resume=<iteration> continues from that dump."""
+    if resume is None:
+        check(lib().rrg_run(str(work_dir).encode(), int(device), PREC[precision]))
+    else:
+        check(lib().rrg_run_resume(str(work_dir).encode(), int(resume), int(device),
+                                   PREC[precision]))
+
+
+def read_wave_state(path, nx: int):
+    cur, prev = np.empty(nx ** 3), np.empty(nx ** 3)
+    t = C.c_double()
+    check(lib().rrg_read_wave_state(str(path).encode(), int(nx), C.byref(t), _d(cur), _d(prev)))
+    return t.value, cur, prev
 
 
 def generate_plummer(seed: int, n: int, total_mass: float = 1.0, scale_radius: float = 1.0,

@@ -665,7 +665,7 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         const size_t sb = direct_scratch_bytes(ctx->prec, n, ctx->splits);
         if (sb) ctx->scratch.alloc(sb);
         const int rb = conservation_blocks(n);
-        ctx->red_partial.alloc(static_cast<size_t>(rb) * 12 * sizeof(double));
+        ctx->red_partial.alloc(static_cast<size_t>(rb) * 12 * 2 * sizeof(double));  // (hi, lo)
         ctx->red_out.alloc(16 * sizeof(double));
         if (layout() != before || n != n_before || ctx->shift_s != shift_before ||
             ctx->uniform_hsoft != hsoft_before || ctx->soft_uniform != uniform_before)
@@ -1071,6 +1071,69 @@ RRG_API rrg_status rrg_solver_precalc(rrg_ctx* ctx) {
             direct(ctx, true, e);
         }
         RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+// Precalc for a state restored from a snapshot (and, in wave mode, from its wave state): the
+// forces come from the restored positions and potential without the setup relaxation, so the
+// next step starts where the saved run stood.
+RRG_API rrg_status rrg_solver_resume(rrg_ctx* ctx) {
+    RRG_ENTRY(ctx, {
+        drop_pending(ctx);
+        RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
+        if (ctx->wave_mode) {
+            deposit_operator(ctx);
+            set_periodic(ctx, 1.0, 0);  // as precalc: rrgsim_integration_rect.cuh:65
+            gradient(ctx);
+        } else {
+            DirectEpi e;
+            e.mode = EPI_STORE;
+            e.acc = ctx->acc.p;
+            e.pot = ctx->pot.p;
+            direct(ctx, true, e);
+        }
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+namespace {
+void copy_level(rrg_ctx* ctx, void* dev, double* host_out, const double* host_in) {
+    const size_t nc = static_cast<size_t>(ctx->grid.nx) * ctx->grid.nx * ctx->grid.nx;
+    if (ctx->rsz == 8) {
+        if (host_out) RRG_CUDA(cudaMemcpy(host_out, dev, nc * 8, cudaMemcpyDeviceToHost));
+        else RRG_CUDA(cudaMemcpy(dev, host_in, nc * 8, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(nc);
+        if (host_out) {
+            RRG_CUDA(cudaMemcpy(f.data(), dev, nc * 4, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < nc; ++i) host_out[i] = f[i];
+        } else {
+            for (size_t i = 0; i < nc; ++i) f[i] = static_cast<float>(host_in[i]);
+            RRG_CUDA(cudaMemcpy(dev, f.data(), nc * 4, cudaMemcpyHostToDevice));
+        }
+    }
+}
+}  // namespace
+
+RRG_API rrg_status rrg_get_wave_state(rrg_ctx* ctx, double* phi_cur, double* phi_prev) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        RRG_REQUIRE(phi_cur && phi_prev, RRG_ERR_INVALID, "rrg_get_wave_state: NULL");
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        copy_level(ctx, ctx->phi[ctx->phi_cur].p, phi_cur, nullptr);
+        copy_level(ctx, ctx->phi[1 - ctx->phi_cur].p, phi_prev, nullptr);
+    })
+}
+
+RRG_API rrg_status rrg_set_wave_state(rrg_ctx* ctx, const double* phi_cur,
+                                      const double* phi_prev) {
+    RRG_ENTRY(ctx, {
+        drop_pending(ctx);
+        require_grid(ctx);
+        RRG_REQUIRE(phi_cur && phi_prev, RRG_ERR_INVALID, "rrg_set_wave_state: NULL");
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        copy_level(ctx, ctx->phi[ctx->phi_cur].p, nullptr, phi_cur);
+        copy_level(ctx, ctx->phi[1 - ctx->phi_cur].p, nullptr, phi_prev);
     })
 }
 

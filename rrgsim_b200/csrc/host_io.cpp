@@ -451,6 +451,47 @@ RRG_API rrg_status rrg_read_dump(const char* path, int64_t capacity, int64_t* n,
     return RRG_OK;
 }
 
+// Wave state beside a snapshot: W_{iter:>5d}.bin = uint64 nx; float64 time;
+// float64 phi_cur[nx^3]; float64 phi_prev[nx^3] (x fastest).
+RRG_API rrg_status rrg_write_wave_state(const char* dump_dir, uint64_t iter, double time,
+                                        int32_t nx, const double* phi_cur,
+                                        const double* phi_prev) {
+    if (!dump_dir || nx < 1 || !phi_cur || !phi_prev)
+        return io_fail(RRG_ERR_INVALID, "rrg_write_wave_state: bad argument");
+    char name[64];
+    std::snprintf(name, sizeof(name), "W_%5llu.bin", static_cast<unsigned long long>(iter));
+    const std::string path = std::string(dump_dir) + "/" + name;
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return io_fail(RRG_ERR_IO, "Can't write wave state: cannot open " + path);
+    const uint64_t N = static_cast<uint64_t>(nx);
+    const size_t nc = static_cast<size_t>(nx) * nx * nx;
+    bool ok = std::fwrite(&N, 8, 1, f) == 1 && std::fwrite(&time, 8, 1, f) == 1 &&
+              std::fwrite(phi_cur, 8, nc, f) == nc && std::fwrite(phi_prev, 8, nc, f) == nc;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? RRG_OK : io_fail(RRG_ERR_IO, "Can't write wave state: short write to " + path);
+}
+
+RRG_API rrg_status rrg_read_wave_state(const char* path, int32_t nx, double* time,
+                                       double* phi_cur, double* phi_prev) {
+    if (!path || nx < 1 || !phi_cur || !phi_prev)
+        return io_fail(RRG_ERR_INVALID, "rrg_read_wave_state: bad argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return io_fail(RRG_ERR_IO, std::string("Can't read wave state: ") + path);
+    uint64_t N = 0;
+    double t = 0;
+    bool ok = std::fread(&N, 8, 1, f) == 1 && std::fread(&t, 8, 1, f) == 1;
+    if (ok && N != static_cast<uint64_t>(nx)) {
+        std::fclose(f);
+        return io_fail(RRG_ERR_INVALID, std::string("wave state grid size differs: ") + path);
+    }
+    const size_t nc = static_cast<size_t>(nx) * nx * nx;
+    ok = ok && std::fread(phi_cur, 8, nc, f) == nc && std::fread(phi_prev, 8, nc, f) == nc;
+    std::fclose(f);
+    if (!ok) return io_fail(RRG_ERR_IO, std::string("Can't read wave state: truncated ") + path);
+    if (time) *time = t;
+    return RRG_OK;
+}
+
 }  // extern "C"
 
 // ================================================================================================

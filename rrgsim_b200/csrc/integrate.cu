@@ -54,19 +54,52 @@ __global__ void correct_kernel(int64_t n, V4<R>* __restrict__ vel, const V4<R>* 
 constexpr int kRedThreads = 256;
 constexpr int kRedVals = 12;
 
-__device__ __forceinline__ double warp_sum(double v) {
+// The sums are double-double (Knuth TwoSum / Fast2Sum carried through every addition, rounded
+// once at the end): each result is the correctly rounded sum of the per-particle terms unless
+// that exact sum lies within about 2^-100 of its magnitude of a rounding boundary, so it does
+// not depend on the order of the particles in memory, which the cell sort changes.
+struct DD {
+    double hi, lo;
+};
+
+__device__ __forceinline__ DD dd_norm(double s, double e) {
+    const double hi = __dadd_rn(s, e);
+    return DD{hi, __dsub_rn(e, __dsub_rn(hi, s))};
+}
+
+__device__ __forceinline__ DD dd_add(DD a, double b) {
+    const double s = __dadd_rn(a.hi, b);
+    const double bb = __dsub_rn(s, a.hi);
+    const double e = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+    return dd_norm(s, __dadd_rn(e, a.lo));
+}
+
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+    const double s = __dadd_rn(a.hi, b.hi);
+    const double bb = __dsub_rn(s, a.hi);
+    const double e = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bb)), __dsub_rn(b.hi, bb));
+    return dd_norm(s, __dadd_rn(e, __dadd_rn(a.lo, b.lo)));
+}
+
+__device__ __forceinline__ DD warp_sum_dd(DD v) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    for (int o = 16; o > 0; o >>= 1) {
+        DD w;
+        w.hi = __shfl_down_sync(0xffffffffu, v.hi, o);
+        w.lo = __shfl_down_sync(0xffffffffu, v.lo, o);
+        v = dd_add(v, w);
+    }
     return v;
 }
 
+// partial: [nblocks][kRedVals][2] (hi, lo)
 template <typename R, bool MIXED>
 __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
     int64_t n, const V4<R>* __restrict__ posm, const V4<float>* __restrict__ lo,
     const V4<R>* __restrict__ vel, const R* __restrict__ pot, double* __restrict__ partial) {
-    double acc[kRedVals];
+    DD acc[kRedVals];
 #pragma unroll
-    for (int k = 0; k < kRedVals; ++k) acc[k] = 0.0;
+    for (int k = 0; k < kRedVals; ++k) acc[k] = DD{0.0, 0.0};
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const V4<R> p = posm[i];
@@ -80,44 +113,49 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
         const double m = p.w;
         const V4<R> v = vel[i];
         const double vx = v.x, vy = v.y, vz = v.z;
-        acc[0] += m * (vx * vx + vy * vy + vz * vz);
-        acc[1] += pot ? m * static_cast<double>(pot[i]) : 0.0;
-        acc[2] += m * vx;
-        acc[3] += m * vy;
-        acc[4] += m * vz;
-        acc[5] += m * (vz * y - vy * z);
-        acc[6] += m * (vx * z - vz * x);
-        acc[7] += m * (vy * x - vx * y);
-        acc[8] += m;
-        acc[9] += m * x;
-        acc[10] += m * y;
-        acc[11] += m * z;
+        acc[0] = dd_add(acc[0], m * (vx * vx + vy * vy + vz * vz));
+        acc[1] = dd_add(acc[1], pot ? m * static_cast<double>(pot[i]) : 0.0);
+        acc[2] = dd_add(acc[2], m * vx);
+        acc[3] = dd_add(acc[3], m * vy);
+        acc[4] = dd_add(acc[4], m * vz);
+        acc[5] = dd_add(acc[5], m * (vz * y - vy * z));
+        acc[6] = dd_add(acc[6], m * (vx * z - vz * x));
+        acc[7] = dd_add(acc[7], m * (vy * x - vx * y));
+        acc[8] = dd_add(acc[8], m);
+        acc[9] = dd_add(acc[9], m * x);
+        acc[10] = dd_add(acc[10], m * y);
+        acc[11] = dd_add(acc[11], m * z);
     }
-    __shared__ double s[kRedThreads / 32][kRedVals];
+    __shared__ DD s[kRedThreads / 32][kRedVals];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < kRedVals; ++k) {
-        const double t = warp_sum(acc[k]);
+        const DD t = warp_sum_dd(acc[k]);
         if (lane == 0) s[w][k] = t;
     }
     __syncthreads();
     if (threadIdx.x < kRedVals) {
-        double t = 0.0;
-        for (int ww = 0; ww < kRedThreads / 32; ++ww) t += s[ww][threadIdx.x];
-        partial[static_cast<int64_t>(blockIdx.x) * kRedVals + threadIdx.x] = t;
+        DD t{0.0, 0.0};
+        for (int ww = 0; ww < kRedThreads / 32; ++ww) t = dd_add(t, s[ww][threadIdx.x]);
+        const int64_t o = (static_cast<int64_t>(blockIdx.x) * kRedVals + threadIdx.x) * 2;
+        partial[o] = t.hi;
+        partial[o + 1] = t.lo;
     }
 }
 
 // One warp per reduced value: lane l sums blocks l, l + 32, ... in order, then a fixed
-// shuffle tree (deterministic).
+// shuffle tree, all in double-double; the result is its rounded high part.
 __global__ void conservation_finish(const double* __restrict__ partial, int nblocks,
                                     double* __restrict__ out) {
     const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (k >= kRedVals) return;
-    double t = 0.0;
-    for (int b = lane; b < nblocks; b += 32) t += partial[static_cast<int64_t>(b) * kRedVals + k];
-    t = warp_sum(t);
-    if (lane == 0) out[k] = t;
+    DD t{0.0, 0.0};
+    for (int b = lane; b < nblocks; b += 32) {
+        const int64_t o = (static_cast<int64_t>(b) * kRedVals + k) * 2;
+        t = dd_add(t, DD{partial[o], partial[o + 1]});
+    }
+    t = warp_sum_dd(t);
+    if (lane == 0) out[k] = t.hi;
 }
 
 // Host FP64 AoS -> device state.

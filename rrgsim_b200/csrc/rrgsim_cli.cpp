@@ -1,4 +1,5 @@
-// `rrgsim <work_dir>`: the solver executable (solver/app/src/rrgsim.cu:12-62).
+// `rrgsim <work_dir> [--resume <iteration>]`: the solver executable
+// (solver/app/src/rrgsim.cu:12-62); --resume continues from dump/S_{iteration:>5d}.bin.
 // Device and arithmetic come from the environment: RRGSIM_DEVICE (default 0) and
 // RRGSIM_PRECISION = fp32 (default) | mixed | fp64.
 #include <cstdio>
@@ -8,8 +9,15 @@
 #include "rrg.h"
 
 int main(int argc, const char** argv) {
-    if (argc < 2) {
-        std::fprintf(stderr, "usage: rrgsim <work_dir>\n");
+    bool resume = false;
+    unsigned long long resume_iter = 0;
+    if (argc == 4 && !std::strcmp(argv[2], "--resume")) {
+        char* end = nullptr;
+        resume_iter = std::strtoull(argv[3], &end, 10);
+        resume = end && *end == '\0' && argv[3][0] != '\0';
+    }
+    if (argc < 2 || (argc > 2 && !resume)) {
+        std::fprintf(stderr, "usage: rrgsim <work_dir> [--resume <iteration>]\n");
         return 1;
     }
     int device = 0;
@@ -23,7 +31,8 @@ int main(int argc, const char** argv) {
             return 1;
         }
     }
-    const rrg_status s = rrg_run(argv[1], device, precision);
+    const rrg_status s = resume ? rrg_run_resume(argv[1], resume_iter, device, precision)
+                                : rrg_run(argv[1], device, precision);
     if (s != RRG_OK) {
         std::fprintf(stderr, "rrgsim: %s\n", rrg_last_error(nullptr));
         return 1;

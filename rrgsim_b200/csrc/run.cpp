@@ -75,13 +75,14 @@ struct Table {
 struct CsvWriter {
     fs::path data_dir;
     std::set<std::string> filled;
+    bool keep_existing = false;  // a resumed run appends to the tables its first part wrote
     void append(const std::string& tag, const std::vector<Table>& items,
                 const std::string& subdir = std::string()) {
         fs::path dir = subdir.empty() ? data_dir : data_dir / subdir;
         std::error_code ec;
         fs::create_directories(dir, ec);
         const fs::path path = dir / (tag + ".csv");
-        const bool first = filled.insert(tag).second;
+        const bool first = filled.insert(tag).second && !(keep_existing && fs::exists(path));
         FILE* f = std::fopen(path.c_str(), first ? "wb" : "ab");
         if (!f) throw std::runtime_error("cannot write " + path.string());
         if (first) {
@@ -231,18 +232,53 @@ struct CtxGuard {
         }                                                                                     \
     } while (0)
 
-}  // namespace
+// The base conservation of a run (its t = 0 state) beside the dumps, so that a resumed run
+// reports the same relative drifts: 9 float64 (time, Ek, Ep, P[3], L[3]).
+bool write_base(const fs::path& dump_dir, const rrg_conservation& c) {
+    FILE* f = std::fopen((dump_dir / "C0.bin").c_str(), "wb");
+    if (!f) return false;
+    const double v[9] = {c.time, c.Ek, c.Ep, c.momentum[0], c.momentum[1], c.momentum[2],
+                         c.angular[0], c.angular[1], c.angular[2]};
+    const bool ok = std::fwrite(v, 8, 9, f) == 9;
+    return (std::fclose(f) == 0) && ok;
+}
 
-extern "C" RRG_API rrg_status rrg_run(const char* work_dir, int device, int precision) {
+bool read_base(const fs::path& dump_dir, rrg_conservation& c) {
+    FILE* f = std::fopen((dump_dir / "C0.bin").c_str(), "rb");
+    if (!f) return false;
+    double v[9];
+    const bool ok = std::fread(v, 8, 9, f) == 9;
+    std::fclose(f);
+    if (!ok) return false;
+    c.time = v[0];
+    c.Ek = v[1];
+    c.Ep = v[2];
+    for (int k = 0; k < 3; ++k) {
+        c.momentum[k] = v[3 + k];
+        c.angular[k] = v[6 + k];
+    }
+    return true;
+}
+
+rrg_status run_impl(const char* work_dir, int device, int precision, bool resume,
+                    uint64_t resume_iter) {
     if (!work_dir) return RRG_ERR_INVALID;
     const fs::path work(work_dir);
     g_log.open(work / "logs");
     CsvWriter csv;
     csv.data_dir = work / "data";
-    {
+    csv.keep_existing = resume;
+    if (!resume) {
         std::error_code ec;
         fs::remove_all(csv.data_dir, ec);  // IOHandler::setup wipes data/ (io_handler.cpp:14)
     }
+    const fs::path dump_dir = work / "dump";
+    auto dump_name = [&](const char* prefix, uint64_t it) {
+        char name[64];
+        std::snprintf(name, sizeof(name), "%s_%5llu.bin", prefix,
+                      static_cast<unsigned long long>(it));
+        return (dump_dir / name).string();
+    };
     CtxGuard guard;
     try {
         rrg_parsed_params pp;
@@ -292,6 +328,25 @@ extern "C" RRG_API rrg_status rrg_run(const char* work_dir, int device, int prec
         }
         log_info("%lld particles loaded", static_cast<long long>(have));
 
+        double time0 = 0.0;
+        if (resume) {
+            // read_particles_dump (io_particles_bin.cu:39-77): positions, velocities and time;
+            // masses and softening stay those of the ICs
+            const std::string sp = dump_name("S", resume_iter);
+            int64_t nd = 0;
+            if (rrg_read_dump(sp.c_str(), have, &nd, &time0, pos.data(), vel.data()) != RRG_OK) {
+                log_error("Error: %s", rrg_last_error(nullptr));
+                return RRG_ERR_IO;
+            }
+            if (nd != have) {
+                log_error("Error: %s holds %lld particles, the ICs %lld", sp.c_str(),
+                          static_cast<long long>(nd), static_cast<long long>(have));
+                rrg::set_thread_error("dump and ICs differ in particle count");
+                return RRG_ERR_INVALID;
+            }
+            log_info("resuming from %s (t = %.10f)", sp.c_str(), time0);
+        }
+
         RUN_CHECK(rrg_create(device, precision, &guard.c));
         RUN_CHECK(rrg_load_particles(guard.c, have, pos.data(), vel.data(), mass.data(),
                                      soft2.data()));
@@ -301,29 +356,59 @@ extern "C" RRG_API rrg_status rrg_run(const char* work_dir, int device, int prec
         }
         if (pp.has_wave) RUN_CHECK(rrg_set_wave_params(guard.c, &pp.wave));
         RUN_CHECK(rrg_solver_init(guard.c, &pp.sim));
-        RUN_CHECK(rrg_solver_precalc(guard.c));
+        const bool wave = pp.sim.use_wave_model != 0;
+        const size_t ncells =
+            pp.has_grid ? static_cast<size_t>(pp.grid.nx) * pp.grid.nx * pp.grid.nx : 0;
+        if (resume) {
+            if (wave) {
+                std::vector<double> cur(ncells), prev(ncells);
+                const std::string wp = dump_name("W", resume_iter);
+                if (rrg_read_wave_state(wp.c_str(), pp.grid.nx, nullptr, cur.data(),
+                                        prev.data()) != RRG_OK) {
+                    log_error("Error: %s", rrg_last_error(nullptr));
+                    return RRG_ERR_IO;
+                }
+                RUN_CHECK(rrg_set_wave_state(guard.c, cur.data(), prev.data()));
+            }
+            RUN_CHECK(rrg_solver_resume(guard.c));
+        } else {
+            RUN_CHECK(rrg_solver_precalc(guard.c));
+        }
         RUN_CHECK(rrg_solver_sync(guard.c));
 
-        const int64_t n = have;
-        std::vector<double> acc(3 * n), grav(n);
-        rrg_conservation c0;
-        RUN_CHECK(rrg_get_particles(guard.c, pos.data(), vel.data(), acc.data(), grav.data()));
-        RUN_CHECK(rrg_calc_conservation(guard.c, &c0));
-        c0.time = 0.0;
-        log_info("base conservation: Ek=%.15f Ep=%.15f", c0.Ek, c0.Ep);
-        save_sample(csv, pos, vel, acc, grav);
-        if (pp.has_grid) save_grid_profiles(csv, guard.c, pp.grid, 0.0);
-
-        const fs::path dump_dir = work / "dump";
         {
             std::error_code ec;
             fs::create_directories(dump_dir, ec);
         }
+        const int64_t n = have;
+        std::vector<double> acc(3 * n), grav(n);
+        rrg_conservation c0;
+        RUN_CHECK(rrg_get_particles(guard.c, pos.data(), vel.data(), acc.data(), grav.data()));
+        if (resume && read_base(dump_dir, c0)) {
+            log_info("base conservation from C0.bin: Ek=%.15f Ep=%.15f", c0.Ek, c0.Ep);
+        } else {
+            RUN_CHECK(rrg_calc_conservation(guard.c, &c0));
+            c0.time = time0;
+            log_info("base conservation: Ek=%.15f Ep=%.15f", c0.Ek, c0.Ep);
+            if (!write_base(dump_dir, c0)) log_error("cannot write %s/C0.bin", dump_dir.c_str());
+        }
+        if (!resume) {
+            save_sample(csv, pos, vel, acc, grav);
+            if (pp.has_grid) save_grid_profiles(csv, guard.c, pp.grid, 0.0);
+        }
+
         const double dt = pp.sim.dt_dynamics;
-        uint64_t iteration = 0;
-        double time = 0.0;
-        double next_save = time + pp.sim.dt_save;
+        uint64_t iteration = resume ? resume_iter : 0;
+        double time = time0;
+        // the save cadence up to `time`, accumulated as the first part of the run did (one
+        // save, and one dt_save increment, per save interval)
+        double next_save = 0.0 + pp.sim.dt_save;
         uint64_t saves_without_dump = 0;
+        while (resume && time >= next_save && pp.sim.dt_save > 0) {
+            next_save += pp.sim.dt_save;
+            ++saves_without_dump;
+        }
+        std::vector<double> wcur(wave ? ncells : 0), wprev(wave ? ncells : 0);
         while (time < pp.sim.time_max) {
             // steps until the next save or the end, accumulated exactly as the reference does
             int k = 0;
@@ -356,6 +441,13 @@ extern "C" RRG_API rrg_status rrg_run(const char* work_dir, int device, int prec
                     if (rrg_write_dump(dump_dir.c_str(), iteration, time, n, pos.data(),
                                        vel.data()) != RRG_OK)
                         log_error("%s", rrg_last_error(nullptr));
+                    if (wave) {
+                        // the wave levels beside the snapshot, for an exact resume
+                        RUN_CHECK(rrg_get_wave_state(guard.c, wcur.data(), wprev.data()));
+                        if (rrg_write_wave_state(dump_dir.c_str(), iteration, time, pp.grid.nx,
+                                                 wcur.data(), wprev.data()) != RRG_OK)
+                            log_error("%s", rrg_last_error(nullptr));
+                    }
                 }
             }
         }
@@ -367,4 +459,15 @@ extern "C" RRG_API rrg_status rrg_run(const char* work_dir, int device, int prec
         return RRG_ERR_IO;
     }
     return RRG_OK;
+}
+
+}  // namespace
+
+extern "C" RRG_API rrg_status rrg_run(const char* work_dir, int device, int precision) {
+    return run_impl(work_dir, device, precision, false, 0);
+}
+
+extern "C" RRG_API rrg_status rrg_run_resume(const char* work_dir, uint64_t iteration,
+                                             int device, int precision) {
+    return run_impl(work_dir, device, precision, true, iteration);
 }

@@ -171,6 +171,26 @@ def test_conservation_reductions(prec):
     assert abs(mt - rm) <= 1e-12
 
 
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_conservation_sums_do_not_depend_on_particle_order(prec):
+    """The reductions are double-double and round once, so the order of the particles in
+    memory (which the cell sort changes) does not change a bit of the result."""
+    n = 20000
+    pos, vel, m, s2 = plummer(n, seed=9)
+    m = m * np.linspace(0.5, 1.5, n)
+    perm = np.random.default_rng(4).permutation(n)
+    out = []
+    for order in (np.arange(n), perm):
+        with _ctx(prec, pos[order], vel[order], m[order], s2[order]) as c:
+            out.append((c.calc_conservation(), c.calc_mass_center()))
+    (a, (ca, ma)), (b, (cb, mb)) = out
+    assert a["Ek"] == b["Ek"]
+    np.testing.assert_array_equal(a["momentum"], b["momentum"])
+    np.testing.assert_array_equal(a["angular"], b["angular"])
+    np.testing.assert_array_equal(ca, cb)
+    assert ma == mb
+
+
 def test_asynchronous_conservation_sums_equal_the_synchronous_ones():
     n = 3000
     pos, vel, m, s2 = plummer(n, seed=8)

@@ -29,8 +29,8 @@ def _write_case(tmp_path, pos, vel, sim, grid=None, wave=None, soft=0.01):
     (tmp_path / "params.json").write_text(json.dumps(params, indent=2))
 
 
-def _run(tmp_path, precision="fp32"):
-    r = subprocess.run([str(rg.BIN_PATH), str(tmp_path)], capture_output=True, text=True,
+def _run(tmp_path, precision="fp32", extra=()):
+    r = subprocess.run([str(rg.BIN_PATH), str(tmp_path), *extra], capture_output=True, text=True,
                        env={"RRGSIM_QUIET": "1", "RRGSIM_PRECISION": precision,
                             "PATH": "/usr/bin:/bin"}, timeout=600)
     assert r.returncode == 0, r.stderr
@@ -50,7 +50,7 @@ def test_rrgsim_nbody_dumps_match_oracle(tmp_path):
     _write_case(tmp_path, pos, vel, {"time_max": 0.02, "dt_save": 0.005, "dt_dynamics": dt,
                                      "saves_without_dump": 3})
     _run(tmp_path)
-    dumps = sorted(p.name for p in (tmp_path / "dump").iterdir())
+    dumps = sorted(p.name for p in (tmp_path / "dump").iterdir() if p.name.startswith("S_"))
     # saves at iterations 5, 10, 15, 20; dumps while the save counter is below 3
     assert dumps == ["S_    5.bin", "S_   10.bin"]
     acc = orc.direct_acc(pos, m, s2)
@@ -86,7 +86,8 @@ def test_rrgsim_wave_mode_runs_and_matches_library(tmp_path):
                 grid={"nx": nx, "dx": dx, "bc_frac": 0.2}, wave=wave, soft=0.01)
     _run(tmp_path)
     names = sorted(p.name for p in (tmp_path / "dump").iterdir())
-    assert names == ["S_    2.bin", "S_    4.bin"]
+    # snapshots, the wave levels beside them, the base conservation
+    assert names == ["C0.bin", "S_    2.bin", "S_    4.bin", "W_    2.bin", "W_    4.bin"]
     # same run through the library API
     grid = rg.GridInfo.from_values(nx, dx, 0.2)
     wp = rg.WaveParams.make(dx, diss_base=wave["diss_base"], wave_speed=c, iterations=20,
@@ -107,3 +108,42 @@ def test_rrgsim_wave_mode_runs_and_matches_library(tmp_path):
     np.testing.assert_array_equal(dv, s["vel"])
     for sub in ("a_grid", "grav_grid", "mass_grid"):
         assert any((tmp_path / "data" / sub).iterdir())
+
+
+@pytest.mark.parametrize("mode,precision", [("nbody", "fp32"), ("wave", "fp32"),
+                                            ("wave", "mixed")])
+def test_resume_from_dump_continues_bit_exactly(tmp_path, mode, precision):
+    """A run to t = 0.0161 and a run to t = 0.0081 resumed from its iteration-4 dump with
+    `--resume 4` produce the same later snapshots, wave levels and conservation tables."""
+    dt = 2e-3
+    if mode == "nbody":
+        pos, vel, _, _ = plummer(1024, seed=31)
+        extra = {}
+    else:
+        pos, vel, _, _ = disk(8192, seed=32)
+        c = 10.0 * float(np.max(np.linalg.norm(vel, axis=1)))
+        extra = {"grid": {"nx": 16, "dx": 1.0, "bc_frac": 0.2},
+                 "wave": {"diss_base": 0.25, "diss_extra": 0.0, "wave_speed": c,
+                          "setup_iterations": 300, "iterations": 20,
+                          "steady_check_step": 1000}}
+    sim = {"dt_save": 0.004, "dt_dynamics": dt, "saves_without_dump": 100}
+    full, part = tmp_path / "full", tmp_path / "part"
+    full.mkdir()
+    part.mkdir()
+    _write_case(full, pos, vel, dict(sim, time_max=0.0161), **extra)
+    _run(full, precision)
+    _write_case(part, pos, vel, dict(sim, time_max=0.0081), **extra)
+    _run(part, precision)
+    assert not (part / "dump" / "S_    6.bin").exists()
+    (part / "params.json").write_text((full / "params.json").read_text())
+    _run(part, precision, extra=("--resume", "4"))
+    for it in (6, 8):
+        a = (full / "dump" / f"S_    {it}.bin").read_bytes()
+        b = (part / "dump" / f"S_    {it}.bin").read_bytes()
+        assert a == b, f"snapshot {it} differs"
+        if mode == "wave":
+            assert (full / "dump" / f"W_    {it}.bin").read_bytes() == \
+                (part / "dump" / f"W_    {it}.bin").read_bytes()
+    for tab in ("delta_energy", "delta_momentum", "delta_ang_z"):
+        assert (full / "data" / f"{tab}.csv").read_text() == \
+            (part / "data" / f"{tab}.csv").read_text(), tab

@@ -78,7 +78,7 @@ def _wave_setup(nx, prec, seed=11):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
-@pytest.mark.parametrize("nx", [8, 33, 64])
+@pytest.mark.parametrize("nx", [8, 33, 64, 128])
 def test_wave_iteration_matches_oracle(prec, nx):
     pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, prec)
     with _ctx(prec, pos, vel, m, s2, g) as c:

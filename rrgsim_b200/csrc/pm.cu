@@ -221,7 +221,7 @@ __device__ __forceinline__ void block_max_to(double dmax, double amax, int tid,
         dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, o));
         amax = fmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
     }
-    __shared__ double sd[kTX * kTY / 32], sa[kTX * kTY / 32];
+    __shared__ double sd[kTX * kTY / 32], sa[kTX * kTY / 32];  // blocks of up to 256 threads
     const int lane = tid & 31, wid = tid >> 5;
     if (lane == 0) {
         sd[wid] = dmax;
@@ -230,7 +230,8 @@ __device__ __forceinline__ void block_max_to(double dmax, double amax, int tid,
     __syncthreads();
     if (tid == 0) {
         double d = 0, a = 0;
-        for (int k = 0; k < kTX * kTY / 32; ++k) {
+        const int warps = static_cast<int>((blockDim.x * blockDim.y + 31) / 32);
+        for (int k = 0; k < warps; ++k) {
             d = fmax(d, sd[k]);
             a = fmax(a, sa[k]);
         }
@@ -296,8 +297,8 @@ __global__ void __launch_bounds__(kTX* kTY, 8) wave_periodic_kernel(
 // planes. About 1.5 memory instructions per cell instead of 7. Same arithmetic as
 // wave_periodic_kernel: lap = x- + x+ + y- + y+ + z- + z+, out = lap K_MAIN + phi K_ACTUAL +
 // phi_old K_OLD + src K_F.
-template <int ZC, bool CHECK>
-__global__ void __launch_bounds__(256, 4) wave_periodic_x4_kernel(
+template <int ZC, bool CHECK, int BS>
+__global__ void __launch_bounds__(BS, 1024 / BS) wave_periodic_x4_kernel(
     const float* __restrict__ phi, float* __restrict__ phi_old, const float* __restrict__ src,
     const WaveDev w, unsigned long long* __restrict__ maxbits) {
     const int nx = w.nx;
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(256, 4) wave_periodic_x4_kernel(
     const int plane4 = W * nx;   // float4 per plane
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int g = blockIdx.x * 256 + tid;  // float4 index within a plane
+    const int g = blockIdx.x * BS + tid;  // float4 index within a plane
     const bool valid = g < plane4;
     const int y = g / W, q = g - (g / W) * W;
     int lsrc, rsrc;
@@ -760,6 +761,15 @@ void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int s
     RRG_LAUNCHED();
 }
 
+// RRG_WAVE_BS = 128 / 256 fixes the block size of the float4 stencil (for sweeps).
+int wave_bs_override() {
+    static const int v = [] {
+        const char* e = std::getenv("RRG_WAVE_BS");
+        return e ? std::atoi(e) : 0;
+    }();
+    return v;
+}
+
 // RRG_WAVE_ZC = 2 / 4 / 8 fixes the z-chunk of the float4 stencil (for sweeps).
 int wave_zc_override() {
     static const int v = [] {
@@ -821,12 +831,16 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
         (32 % W4 == 0 || W4 % 32 == 0)) {
         // float4 rows: z-chunk of 2, 4 or 8 planes (dividing nx), at least two blocks per SM
         // (at 128^3 that is 4, measured fastest inside the PM step on B200)
-        const int rows_blocks = div_up(static_cast<int64_t>(W4) * nx, 256);
+        // 128-thread blocks: at 128^3 with 4-plane chunks 1024 blocks fill 8 per SM to 99%
+        // (256-thread blocks: 512 on 4 per SM, 86%); measured faster inside the PM step
+        const int bs = wave_bs_override() == 256 ? 256 : 128;
+        const int rows_blocks = div_up(static_cast<int64_t>(W4) * nx, bs);
         int zx = wave_zc_override();
         if (zx != 2 && zx != 4 && zx != 8) {
             zx = 2;
             for (int cand : {8, 4})
-                if (nx % cand == 0 && static_cast<int64_t>(rows_blocks) * (nx / cand) >= 2 * sms) {
+                if (nx % cand == 0 &&
+                    static_cast<int64_t>(rows_blocks) * (nx / cand) * bs >= 2 * 256 * sms) {
                     zx = cand;
                     break;
                 }
@@ -836,15 +850,21 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
         const float* p = static_cast<const float*>(phi);
         float* po = static_cast<float*>(phi_old_inout);
         const float* sr = static_cast<const float*>(src);
-#define RRG_WAVE_X4(Z)                                                                       \
+#define RRG_WAVE_X4B(Z, B)                                                                   \
     do {                                                                                      \
-        if (check) wave_periodic_x4_kernel<Z, true><<<g4, 256, 0, s>>>(p, po, sr, w, maxbits); \
-        else wave_periodic_x4_kernel<Z, false><<<g4, 256, 0, s>>>(p, po, sr, w, maxbits);      \
+        if (check) wave_periodic_x4_kernel<Z, true, B><<<g4, B, 0, s>>>(p, po, sr, w, maxbits); \
+        else wave_periodic_x4_kernel<Z, false, B><<<g4, B, 0, s>>>(p, po, sr, w, maxbits);      \
+    } while (0)
+#define RRG_WAVE_X4(Z)                  \
+    do {                                \
+        if (bs == 128) RRG_WAVE_X4B(Z, 128); \
+        else RRG_WAVE_X4B(Z, 256);      \
     } while (0)
         if (zx == 8) RRG_WAVE_X4(8);
         else if (zx == 4) RRG_WAVE_X4(4);
         else RRG_WAVE_X4(2);
 #undef RRG_WAVE_X4
+#undef RRG_WAVE_X4B
         RRG_LAUNCHED();
         return;
     }

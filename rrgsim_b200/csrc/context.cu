@@ -966,11 +966,11 @@ RRG_API rrg_status rrg_project_grid_grav_on_particles(rrg_ctx* ctx) {
     })
 }
 
-static void reduce_state(rrg_ctx* ctx) {
+static void reduce_state(rrg_ctx* ctx, bool com) {
     const int rb = conservation_blocks(ctx->n);
     launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
                         ctx->red_partial.as<double>(), rb, ctx->red_out.as<double>(),
-                        ctx->stream);
+                        ctx->stream, com);
     RRG_CUDA(cudaMemcpyAsync(ctx->host_red, ctx->red_out.p, 12 * sizeof(double),
                              cudaMemcpyDeviceToHost, ctx->stream));
     RRG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -980,7 +980,7 @@ RRG_API rrg_status rrg_calc_conservation(rrg_ctx* ctx, rrg_conservation* out) {
     RRG_ENTRY(ctx, {
         require_particles(ctx);
         RRG_REQUIRE(out != nullptr, RRG_ERR_INVALID, "NULL output");
-        reduce_state(ctx);
+        reduce_state(ctx, false);
         const double* r = ctx->host_red;
         out->time = ctx->time;
         out->Ek = 0.5 * r[0];
@@ -999,7 +999,7 @@ RRG_API rrg_status rrg_calc_conservation_async(rrg_ctx* ctx, double* sums) {
         const int rb = conservation_blocks(ctx->n);
         launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
                             ctx->red_partial.as<double>(), rb, ctx->red_out.as<double>(),
-                            ctx->stream);
+                            ctx->stream, false);
         RRG_CUDA(cudaMemcpyAsync(sums, ctx->red_out.p, 12 * sizeof(double),
                                  cudaMemcpyDeviceToHost, ctx->stream));
     })
@@ -1022,7 +1022,7 @@ RRG_API rrg_status rrg_calc_mass_center(rrg_ctx* ctx, double center_of_mass[3],
                                         double* total_mass) {
     RRG_ENTRY(ctx, {
         require_particles(ctx);
-        reduce_state(ctx);
+        reduce_state(ctx, true);
         const double* r = ctx->host_red;
         const double M = r[8];
         for (int k = 0; k < 3; ++k)

@@ -48,7 +48,7 @@ __global__ void correct_kernel(int64_t n, V4<R>* __restrict__ vel, const V4<R>* 
 // ---------------------------------------------------------------------------------------------
 // FP64 reductions: per particle (promoted to double)
 //   Ek2 += m v^2, Ep2 += m phi, P += m v, L += m (x cross v), M += m, Mx += m x
-// Block partials are summed by one block in a fixed order (deterministic).
+// Block partials are summed by one block in a fixed order.
 // calc_conservation: nbody.cu:246-291; compute_center_of_mass_kernel: nbody.cu:293-396.
 // ---------------------------------------------------------------------------------------------
 constexpr int kRedThreads = 256;
@@ -92,14 +92,29 @@ __device__ __forceinline__ DD warp_sum_dd(DD v) {
     return v;
 }
 
-// partial: [nblocks][kRedVals][2] (hi, lo)
-template <typename R, bool MIXED>
+// Per thread each sum is cascaded (Ogita, Rump and Oishi's Sum2): s += x by TwoSum, and the
+// rounding errors add up in c, 7 FP64 operations per term; (s, c) becomes a double-double for the
+// warp, block and final reductions. partial: [nblocks][kRedVals][2] (hi, lo). COM adds the four
+// mass-centre sums (M, Mx); without it they stay 0.
+struct Casc {
+    double s, c;
+};
+
+__device__ __forceinline__ void casc_add(Casc& a, double x) {
+    const double t = __dadd_rn(a.s, x);
+    const double z = __dsub_rn(t, a.s);
+    a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, z)), __dsub_rn(x, z)));
+    a.s = t;
+}
+
+template <typename R, bool MIXED, bool COM>
 __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
     int64_t n, const V4<R>* __restrict__ posm, const V4<float>* __restrict__ lo,
     const V4<R>* __restrict__ vel, const R* __restrict__ pot, double* __restrict__ partial) {
-    DD acc[kRedVals];
+    constexpr int NV = COM ? kRedVals : 8;
+    Casc acc[NV];
 #pragma unroll
-    for (int k = 0; k < kRedVals; ++k) acc[k] = DD{0.0, 0.0};
+    for (int k = 0; k < NV; ++k) acc[k] = Casc{0.0, 0.0};
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const V4<R> p = posm[i];
@@ -113,30 +128,33 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
         const double m = p.w;
         const V4<R> v = vel[i];
         const double vx = v.x, vy = v.y, vz = v.z;
-        acc[0] = dd_add(acc[0], m * (vx * vx + vy * vy + vz * vz));
-        acc[1] = dd_add(acc[1], pot ? m * static_cast<double>(pot[i]) : 0.0);
-        acc[2] = dd_add(acc[2], m * vx);
-        acc[3] = dd_add(acc[3], m * vy);
-        acc[4] = dd_add(acc[4], m * vz);
-        acc[5] = dd_add(acc[5], m * (vz * y - vy * z));
-        acc[6] = dd_add(acc[6], m * (vx * z - vz * x));
-        acc[7] = dd_add(acc[7], m * (vy * x - vx * y));
-        acc[8] = dd_add(acc[8], m);
-        acc[9] = dd_add(acc[9], m * x);
-        acc[10] = dd_add(acc[10], m * y);
-        acc[11] = dd_add(acc[11], m * z);
+        casc_add(acc[0], m * (vx * vx + vy * vy + vz * vz));
+        casc_add(acc[1], pot ? m * static_cast<double>(pot[i]) : 0.0);
+        casc_add(acc[2], m * vx);
+        casc_add(acc[3], m * vy);
+        casc_add(acc[4], m * vz);
+        casc_add(acc[5], m * (vz * y - vy * z));
+        casc_add(acc[6], m * (vx * z - vz * x));
+        casc_add(acc[7], m * (vy * x - vx * y));
+        if constexpr (COM) {
+            casc_add(acc[8], m);
+            casc_add(acc[9], m * x);
+            casc_add(acc[10], m * y);
+            casc_add(acc[11], m * z);
+        }
     }
     __shared__ DD s[kRedThreads / 32][kRedVals];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < kRedVals; ++k) {
-        const DD t = warp_sum_dd(acc[k]);
+    for (int k = 0; k < NV; ++k) {
+        const DD t = warp_sum_dd(dd_norm(acc[k].s, acc[k].c));
         if (lane == 0) s[w][k] = t;
     }
     __syncthreads();
     if (threadIdx.x < kRedVals) {
         DD t{0.0, 0.0};
-        for (int ww = 0; ww < kRedThreads / 32; ++ww) t = dd_add(t, s[ww][threadIdx.x]);
+        if (threadIdx.x < NV)
+            for (int ww = 0; ww < kRedThreads / 32; ++ww) t = dd_add(t, s[ww][threadIdx.x]);
         const int64_t o = (static_cast<int64_t>(blockIdx.x) * kRedVals + threadIdx.x) * 2;
         partial[o] = t.hi;
         partial[o + 1] = t.lo;
@@ -256,26 +274,31 @@ void launch_correct(int prec, int64_t n, void* vel, const void* acc, const void*
     RRG_LAUNCHED();
 }
 
+// Two blocks per SM: the sums are FP64-bound, and few partials keep the final pass short.
 int conservation_blocks(int64_t n) {
     const int b = div_up(n, kRedThreads);
-    return b < 1184 ? (b < 1 ? 1 : b) : 1184;
+    return b < 296 ? (b < 1 ? 1 : b) : 296;
 }
 
 void launch_conservation(int prec, int64_t n, const void* posm, const void* poslo,
                          const void* vel, const void* pot, double* partial, int nblocks,
-                         double* out, cudaStream_t s) {
-    if (prec == RRG_PREC_FP64)
-        conservation_kernel<double, false><<<nblocks, kRedThreads, 0, s>>>(
-            n, static_cast<const V4<double>*>(posm), nullptr,
-            static_cast<const V4<double>*>(vel), static_cast<const double*>(pot), partial);
-    else if (prec == RRG_PREC_MIXED)
-        conservation_kernel<float, true><<<nblocks, kRedThreads, 0, s>>>(
-            n, static_cast<const V4<float>*>(posm), static_cast<const V4<float>*>(poslo),
-            static_cast<const V4<float>*>(vel), static_cast<const float*>(pot), partial);
-    else
-        conservation_kernel<float, false><<<nblocks, kRedThreads, 0, s>>>(
-            n, static_cast<const V4<float>*>(posm), nullptr, static_cast<const V4<float>*>(vel),
-            static_cast<const float*>(pot), partial);
+                         double* out, cudaStream_t s, bool com) {
+#define RRG_CONS(R, MX, C, LO)                                                               \
+    conservation_kernel<R, MX, C><<<nblocks, kRedThreads, 0, s>>>(                            \
+        n, static_cast<const V4<R>*>(posm), LO, static_cast<const V4<R>*>(vel),               \
+        static_cast<const R*>(pot), partial)
+    const V4<float>* lo = static_cast<const V4<float>*>(poslo);
+    if (prec == RRG_PREC_FP64) {
+        if (com) RRG_CONS(double, false, true, nullptr);
+        else RRG_CONS(double, false, false, nullptr);
+    } else if (prec == RRG_PREC_MIXED) {
+        if (com) RRG_CONS(float, true, true, lo);
+        else RRG_CONS(float, true, false, lo);
+    } else {
+        if (com) RRG_CONS(float, false, true, nullptr);
+        else RRG_CONS(float, false, false, nullptr);
+    }
+#undef RRG_CONS
     RRG_LAUNCHED();
     conservation_finish<<<1, 32 * kRedVals, 0, s>>>(partial, nblocks, out);
     RRG_LAUNCHED();

@@ -63,12 +63,12 @@ void launch_correct(int prec, int64_t n, void* vel, const void* acc, const void*
                     cudaStream_t s);
 
 // FP64 reductions of the state (calc_conservation, nbody.cu:246-291; centre of mass,
-// nbody.cu:293-439). out[0..11] = Ek2 (sum m v^2), Ep2 (sum m phi), P[3], L[3], M, Mx[3],
-// summed in double-double, so independent of the particles' memory order. partial holds
-// nblocks x 12 x 2 doubles.
+// nbody.cu:293-439). out[0..11] = Ek2 (sum m v^2), Ep2 (sum m phi), P[3], L[3], and with com
+// also M, Mx[3] (else 0), summed in double-double, so independent of the particles' memory order.
+// partial holds nblocks x 12 x 2 doubles.
 void launch_conservation(int prec, int64_t n, const void* posm, const void* poslo,
                          const void* vel, const void* pot, double* partial, int nblocks,
-                         double* out, cudaStream_t s);
+                         double* out, cudaStream_t s, bool com);
 int conservation_blocks(int64_t n);
 
 // Conversions between the host FP64 AoS layout and the device state.

@@ -129,16 +129,18 @@ __global__ void __launch_bounds__(256) cic_kernel(int64_t n, const void* __restr
 // Wave source: f = 4 pi G rho, rho = mass / dx^3 - rho_sub (wave.cu:150-153), mass from the
 // fixed-point grid. Optionally clears the fixed-point grid for the next deposit.
 // ----------------------------------------------------------------------------------------------
+// FP64 divides by dx^3 as the reference does; FP32, whose source is rounded to float anyway,
+// multiplies by the host's 1 / dx^3 (an FP64 division per cell made this pass instruction-bound).
 template <typename R>
 __global__ void wave_source_kernel(int64_t ncells, unsigned long long* __restrict__ mgrid,
-                                   double inv_scale, double dx, double rho_sub, double mult,
-                                   R* __restrict__ src, bool zero_grid) {
+                                   double inv_scale, double dx3, double inv_dx3, double rho_sub,
+                                   double mult, R* __restrict__ src, bool zero_grid) {
     const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     const unsigned long long q = mgrid[c];
     if (zero_grid) mgrid[c] = 0ull;
     const double mass = static_cast<double>(q) * inv_scale;
-    const double rho = mass / (dx * dx * dx) - rho_sub;
+    const double rho = (sizeof(R) == 8 ? mass / dx3 : mass * inv_dx3) - rho_sub;
     src[c] = static_cast<R>(mult * (4.0 * kPi * 1.0 * rho));
 }
 
@@ -508,6 +510,90 @@ __global__ void __launch_bounds__(kTX* kTY) gradient_kernel(int nx, R coef,
     acc4[c] = v4<R>(dx * coef, dy * coef, dz * coef, pc);
 }
 
+// FP32 gradient with four x-cells per thread (float4 rows, as wave_periodic_x4_kernel): x +- 1
+// by warp shuffles (a scalar load at warp edges when a row is wider than a warp), rows y +- 1 as
+// coalesced float4 loads, the z neighbours from a register pipeline over ZC planes, and the four
+// (ax, ay, az, phi) cells written as four float4 stores. Same expressions, faces one-sided, as
+// gradient_kernel. Needs nx % 4 == 0, nx % ZC == 0 and nx / 4 dividing 32 or a multiple of 32.
+template <int ZC, int BS>
+__global__ void __launch_bounds__(BS) gradient_x4_kernel(int nx, float coef,
+                                                         const float* __restrict__ phi,
+                                                         float4* __restrict__ acc4) {
+    const int W = nx >> 2;
+    const int plane4 = W * nx;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int g = blockIdx.x * BS + tid;
+    const bool valid = g < plane4;
+    const int y = g / W, q = g - (g / W) * W;
+    int lsrc, rsrc;
+    bool lload = false, rload = false;
+    if (W >= 32) {
+        lsrc = (lane + 31) & 31;
+        rsrc = (lane + 1) & 31;
+        lload = W > 32 && lane == 0 && q > 0;
+        rload = W > 32 && lane == 31 && q < W - 1;
+    } else {
+        const int seg = lane - lane % W;
+        lsrc = seg + (lane - seg + W - 1) % W;
+        rsrc = seg + (lane - seg + 1) % W;
+    }
+    const float4* phi4 = reinterpret_cast<const float4*>(phi);
+    const int z0 = blockIdx.y * ZC;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 pv[ZC + 2];  // phi at z0 - 1 ... z0 + ZC (clamped to the box; faces are one-sided)
+#pragma unroll
+    for (int k = 0; k < ZC + 2; ++k) {
+        const int z = min(max(z0 - 1 + k, 0), nx - 1);
+        pv[k] = valid ? __ldg(phi4 + g + z * plane4) : zero4;
+    }
+    const int gym = y > 0 ? g - W : g;
+    const int gyp = y < nx - 1 ? g + W : g;
+    const int x = 4 * q;
+#pragma unroll
+    for (int k = 0; k < ZC; ++k) {
+        const int z = z0 + k;
+        const float4 c = pv[k + 1];
+        float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+        float rgt = __shfl_sync(0xffffffffu, c.x, rsrc);
+        if (!valid) continue;
+        const int rowbase = z * nx * nx + y * nx;
+        if (lload) lft = __ldg(phi + rowbase + x - 1);
+        if (rload) rgt = __ldg(phi + rowbase + x + 4);
+        // x: central inside, one-sided at x = 0 and x = nx - 1
+        const float d0 = x == 0 ? c.y - c.x : 0.5f * (c.y - lft);
+        const float d1 = 0.5f * (c.z - c.x);
+        const float d2 = 0.5f * (c.w - c.y);
+        const float d3 = x + 4 == nx ? c.w - c.z : 0.5f * (rgt - c.z);
+        // y
+        float4 ey;
+        if (y == 0) {
+            const float4 yp = __ldg(phi4 + gyp + z * plane4);
+            ey = make_float4(yp.x - c.x, yp.y - c.y, yp.z - c.z, yp.w - c.w);
+        } else if (y == nx - 1) {
+            const float4 ym = __ldg(phi4 + gym + z * plane4);
+            ey = make_float4(c.x - ym.x, c.y - ym.y, c.z - ym.z, c.w - ym.w);
+        } else {
+            const float4 yp = __ldg(phi4 + gyp + z * plane4);
+            const float4 ym = __ldg(phi4 + gym + z * plane4);
+            ey = make_float4(0.5f * (yp.x - ym.x), 0.5f * (yp.y - ym.y), 0.5f * (yp.z - ym.z),
+                             0.5f * (yp.w - ym.w));
+        }
+        // z
+        const float4 zm = pv[k], zp = pv[k + 2];
+        float4 ez;
+        if (z == 0) ez = make_float4(zp.x - c.x, zp.y - c.y, zp.z - c.z, zp.w - c.w);
+        else if (z == nx - 1) ez = make_float4(c.x - zm.x, c.y - zm.y, c.z - zm.z, c.w - zm.w);
+        else
+            ez = make_float4(0.5f * (zp.x - zm.x), 0.5f * (zp.y - zm.y), 0.5f * (zp.z - zm.z),
+                             0.5f * (zp.w - zm.w));
+        float4* o = acc4 + (static_cast<size_t>(z) * nx + y) * nx + x;
+        o[0] = make_float4(d0 * coef, ey.x * coef, ez.x * coef, c.x);
+        o[1] = make_float4(d1 * coef, ey.y * coef, ez.y * coef, c.y);
+        o[2] = make_float4(d2 * coef, ey.z * coef, ez.z * coef, c.z);
+        o[3] = make_float4(d3 * coef, ey.w * coef, ez.w * coef, c.w);
+    }
+}
+
 // ----------------------------------------------------------------------------------------------
 // Trilinear gather (interpolate_acceleration_to_particles_kernel, rm_mesh2p.cu:48-114).
 // Index selection as the reference: f = (x - domain_min) / dx - 0.5 in FP64, i0 = floorf(f)
@@ -752,12 +838,15 @@ void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int s
     const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
     const double inv_scale = ldexp(1.0, -shift_s);
     auto* mg = const_cast<unsigned long long*>(mgrid);
+    const double dx3 = dx * dx * dx;
     if (prec == RRG_PREC_FP64)
         wave_source_kernel<double><<<div_up(nc, 256), 256, 0, s>>>(
-            nc, mg, inv_scale, dx, rho_mean, scale, static_cast<double*>(src), zero_grid);
+            nc, mg, inv_scale, dx3, 1.0 / dx3, rho_mean, scale, static_cast<double*>(src),
+            zero_grid);
     else
         wave_source_kernel<float><<<div_up(nc, 256), 256, 0, s>>>(
-            nc, mg, inv_scale, dx, rho_mean, scale, static_cast<float*>(src), zero_grid);
+            nc, mg, inv_scale, dx3, 1.0 / dx3, rho_mean, scale, static_cast<float*>(src),
+            zero_grid);
     RRG_LAUNCHED();
 }
 
@@ -913,9 +1002,18 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
 }
 
 void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, cudaStream_t s) {
+    const double coef = -1.0 / dx;
+    const int W4 = nx / 4;
+    if (prec != RRG_PREC_FP64 && nx >= 8 && nx % 4 == 0 && (32 % W4 == 0 || W4 % 32 == 0)) {
+        dim3 g4(div_up(static_cast<int64_t>(W4) * nx, 128), nx / 4);
+        gradient_x4_kernel<4, 128><<<g4, 128, 0, s>>>(nx, static_cast<float>(coef),
+                                                      static_cast<const float*>(phi),
+                                                      static_cast<float4*>(acc4));
+        RRG_LAUNCHED();
+        return;
+    }
     dim3 grid(div_up(nx, kTX), div_up(nx, kTY), nx);
     dim3 block(kTX, kTY);
-    const double coef = -1.0 / dx;
     if (prec == RRG_PREC_FP64)
         gradient_kernel<double><<<grid, block, 0, s>>>(nx, coef, static_cast<const double*>(phi),
                                                        static_cast<V4<double>*>(acc4));

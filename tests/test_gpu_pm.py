@@ -154,9 +154,10 @@ def test_steady_state_relaxation(prec):
     assert np.max(np.abs(got["grav"] - ref)) <= (1e-12 if prec == "fp64" else 1e-3) * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("nx", [40, 32, 64, 128])
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
-def test_gradient_and_interpolation(prec):
-    nx = 40
+def test_gradient_and_interpolation(prec, nx):
+    """nx = 40 runs the scalar gradient, 32 / 64 / 128 the float4-row one in FP32 and MIXED."""
     rng = np.random.default_rng(5)
     pos, vel, m, s2 = disk(30000, seed=5)
     pos[:4] = [[9.5, 0, 0], [-8.0, -8.0, -8.0], [7.99, 7.99, 7.99], [0.1, -0.1, 0.2]]

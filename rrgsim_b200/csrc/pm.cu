@@ -82,6 +82,7 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
     const int jj[8] = {j0, j0, j1, j1, j0, j0, j1, j1};
     const int kk[8] = {k0, k0, k0, k0, k1, k1, k1, k1};
     const double wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
+    unsigned sum[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         unsigned q = 0;
@@ -89,10 +90,16 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
             const double w = __dmul_rn(__dmul_rn(wxs[c & 1], wys[(c >> 1) & 1]), wzs[c >> 2]);
             q = static_cast<unsigned>(__double2ll_rn(__dmul_rn(ms, w)));
         }
-        const unsigned s = __reduce_add_sync(peers, q);
-        if (active && leader && s != 0u) {
-            const int64_t a = ii[c] + static_cast<int64_t>(jj[c]) * nx + kk[c] * nx2;
-            atomicAdd(grid + a, static_cast<unsigned long long>(s));
+        sum[c] = __reduce_add_sync(peers, q);
+    }
+    // one divergent branch: the group leader adds the eight corner sums
+    if (active && leader) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            if (sum[c] != 0u) {
+                const int64_t a = ii[c] + static_cast<int64_t>(jj[c]) * nx + kk[c] * nx2;
+                atomicAdd(grid + a, static_cast<unsigned long long>(sum[c]));
+            }
         }
     }
 }
@@ -600,9 +607,12 @@ __global__ void __launch_bounds__(BS) gradient_x4_kernel(int nx, float coef,
 // (the reference passes its double to floorf, i.e. floors the float-rounded value), weights
 // from the unclamped fraction, indices clamped to [0, nx - 1]; summation order z, y, x.
 // ----------------------------------------------------------------------------------------------
-__device__ __forceinline__ void interp_axis(double x, double dmin, double dx, int nx, int& i0,
-                                            int& i1, double& w) {
-    const double f = (x - dmin) / dx - 0.5;
+// DIV: divide by dx as the reference (FP64 path); else multiply by 1 / dx (FP32 and MIXED,
+// whose weights are rounded to float: an FP64 division per axis dominated the particle pass).
+template <bool DIV>
+__device__ __forceinline__ void interp_axis(double x, double dmin, double dx, double inv_dx,
+                                            int nx, int& i0, int& i1, double& w) {
+    const double f = (DIV ? (x - dmin) / dx : (x - dmin) * inv_dx) - 0.5;
     int a = static_cast<int>(floorf(static_cast<float>(f)));
     w = f - a;
     i0 = max(0, min(a, nx - 1));
@@ -614,26 +624,27 @@ __device__ __forceinline__ void trilinear(const V4<R>* __restrict__ acc4, const 
                                           double x, double y, double z, R& ax, R& ay, R& az) {
     int i0, i1, j0, j1, k0, k1;
     double wxd, wyd, wzd;
-    interp_axis(x, g.domain_min, g.dx, g.nx, i0, i1, wxd);
-    interp_axis(y, g.domain_min, g.dx, g.nx, j0, j1, wyd);
-    interp_axis(z, g.domain_min, g.dx, g.nx, k0, k1, wzd);
+    constexpr bool DIV = sizeof(R) == 8;
+    interp_axis<DIV>(x, g.domain_min, g.dx, g.inv_dx, g.nx, i0, i1, wxd);
+    interp_axis<DIV>(y, g.domain_min, g.dx, g.inv_dx, g.nx, j0, j1, wyd);
+    interp_axis<DIV>(z, g.domain_min, g.dx, g.inv_dx, g.nx, k0, k1, wzd);
     const R wx = static_cast<R>(wxd), wy = static_cast<R>(wyd), wz = static_cast<R>(wzd);
-    const int64_t nx = g.nx;
+    const int nx = g.nx;  // nx^3 < 2^31 (nx <= 1024)
     ax = ay = az = R(0);
 #pragma unroll
     for (int k = 0; k <= 1; ++k) {
-        const int64_t kk = k == 0 ? k0 : k1;
+        const int kk = k == 0 ? k0 : k1;
         const R wk = k == 0 ? (R(1) - wz) : wz;
 #pragma unroll
         for (int j = 0; j <= 1; ++j) {
-            const int64_t jj = j == 0 ? j0 : j1;
+            const int jj = j == 0 ? j0 : j1;
             const R wj = j == 0 ? (R(1) - wy) : wy;
 #pragma unroll
             for (int i = 0; i <= 1; ++i) {
-                const int64_t ii = i == 0 ? i0 : i1;
+                const int ii = i == 0 ? i0 : i1;
                 const R wi = i == 0 ? (R(1) - wx) : wx;
                 const R weight = wi * wj * wk;
-                const V4<R> f = acc4[kk * nx * nx + jj * nx + ii];
+                const V4<R> f = acc4[(kk * nx + jj) * nx + ii];
                 ax += weight * f.x;
                 ay += weight * f.y;
                 az += weight * f.z;

@@ -238,6 +238,21 @@ RRG_API rrg_status rrg_solve_wave_equation(rrg_ctx* ctx, int max_iterations,
 
 /* calc_acceleration_field: rm_p2mesh.cu:238-290, 337-354 */
 RRG_API rrg_status rrg_calc_acceleration_field(rrg_ctx* ctx);
+/* No reference counterpart: rrg_solve_wave_equation for exactly `iterations` substeps without
+ * steady-state checks, then rrg_calc_acceleration_field, as one call. Periodic FP32 / MIXED
+ * grids of 32, 64 or 128 cells without an absorbing layer run it as one persistent kernel
+ * (source, substeps and gradient in one launch, the per-step wave solve of the fused stepping
+ * path); everything else launches the separate kernels. The results are the same bits either
+ * way. iterations >= 1. */
+RRG_API rrg_status rrg_solve_wave_and_field(rrg_ctx* ctx, int iterations);
+/* No reference counterpart. The device memory through which the persistent wave solve's thread
+ * blocks synchronise, for diagnostics: per block an epoch counter (uint32, 128 bytes apart,
+ * block = z-chunk x blocks-along-y + y-block), the error word (the uint32 at byte 65532,
+ * non-zero after a wait between blocks ran out), then the face buffers. Zeroed by
+ * rrg_init_grid; writing it makes the next solve report an error (or compute garbage).
+ * Synchronising calls (rrg_synchronize, rrg_get_particles, rrg_calc_conservation) turn a set
+ * error word into RRG_ERR_CUDA and zero the memory again. */
+RRG_API rrg_status rrg_wave_solve_sync(rrg_ctx* ctx, void** dev_ptr, size_t* bytes);
 /* project_grid_acceleration_on_particles: solver/lib/rrgsim_rect_mesh/src/rm_mesh2p.cu:
  * 48-114, 129-152 (trilinear) */
 RRG_API rrg_status rrg_project_grid_acceleration_on_particles(rrg_ctx* ctx);

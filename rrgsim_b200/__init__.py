@@ -133,6 +133,8 @@ def lib() -> C.CDLL:
         "rrg_set_boundary_monopole": (st, [vp, C.c_double, d, i32]),
         "rrg_set_boundary_zero": (st, [vp]),
         "rrg_solve_wave_equation": (st, [vp, i32, C.POINTER(C.c_int), d]),
+        "rrg_solve_wave_and_field": (st, [vp, i32]),
+        "rrg_wave_solve_sync": (st, [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
         "rrg_calc_acceleration_field": (st, [vp]),
         "rrg_project_grid_acceleration_on_particles": (st, [vp]),
         "rrg_project_grid_grav_on_particles": (st, [vp]),
@@ -321,6 +323,19 @@ class Context:
 
     def calc_acceleration_field(self) -> None:
         self._c(lib().rrg_calc_acceleration_field(self._h))
+
+    def solve_wave_and_field(self, iterations: int) -> None:
+        """solve_wave_equation for exactly `iterations` substeps (no steady checks), then
+        calc_acceleration_field, as one call: one persistent kernel on periodic FP32 / MIXED
+        grids of 32, 64 or 128 cells without an absorbing layer."""
+        self._c(lib().rrg_solve_wave_and_field(self._h, int(iterations)))
+
+    def wave_solve_sync(self) -> tuple[int, int]:
+        """(device address, bytes) of the persistent wave solve's synchronisation memory:
+        per-block epoch counters 128 bytes apart, the error word at byte 65532, the faces."""
+        p, n = C.c_void_p(), C.c_size_t()
+        self._c(lib().rrg_wave_solve_sync(self._h, C.byref(p), C.byref(n)))
+        return int(p.value or 0), int(n.value)
 
     def project_grid_acceleration_on_particles(self) -> None:
         self._c(lib().rrg_project_grid_acceleration_on_particles(self._h))

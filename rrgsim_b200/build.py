@@ -32,7 +32,8 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I", str(INCLU
             str(CSRC), "-I", "/usr/local/cuda/include"]
 
 LIB_SOURCES = ["direct.cu", "integrate.cu", "pm.cu", "context.cu", "adjoint.cu", "host_io.cpp",
-               "run.cpp", "noalloc.cu", "sort.cu", "ensemble.cu", "pm_adjoint.cu"]
+               "run.cpp", "noalloc.cu", "sort.cu", "ensemble.cu", "pm_adjoint.cu",
+               "wave_solve.cu"]
 
 
 def _headers() -> list[Path]:

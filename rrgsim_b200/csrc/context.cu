@@ -120,6 +120,8 @@ struct rrg_ctx {
     double bc_mass = 0.0, com[3] = {0, 0, 0}, r_min = 0.0, rho_mean = 0.0;
     int keep_layer = 0;
     Buf maxbits;
+    Buf wsync;                       // the persistent solve's progress counters and error word
+    bool wave_solve_used = false;
 
     // reductions / transfers
     Buf red_partial, red_out, dl;
@@ -256,6 +258,41 @@ void wave_substep(rrg_ctx* c, const WaveCoef& w, unsigned long long* maxbits) {
 
 void gradient(rrg_ctx* c) {
     launch_gradient(c->prec, c->grid.nx, c->grid.dx, c->phi[c->phi_cur].p, c->acc4.p, c->stream);
+}
+
+// The source, `iterations` substeps and the gradient as the persistent kernel, where it applies
+// (FP32 grids, periodic box without an absorbing layer, a grid whose blocks all fit on the GPU
+// at once). The results equal those of wave_source + wave_substep x iterations + gradient;
+// false: nothing launched, the caller launches those.
+bool solve_step_persistent(rrg_ctx* c, const WaveCoef& w, int iterations) {
+    if (c->prec == RRG_PREC_FP64 || c->bc_type != RRG_BC_PERIODIC || c->keep_layer) return false;
+    if (!launch_wave_solve(c->grid.nx, iterations, c->phi[0].as<float>(),
+                           c->phi[1].as<float>(), c->phi_cur,
+                           c->mg[c->mg_cur].as<unsigned long long>(),
+                           c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
+                           c->rho_mean, w, c->src.as<float>(), c->acc4.as<float4>(),
+                           c->wsync.as<unsigned int>(), c->wsync.bytes, c->stream))
+        return false;
+    if (iterations % 2 == 1) c->phi_cur = 1 - c->phi_cur;
+    c->src_dirty = false;
+    c->wave_solve_used = true;
+    return true;
+}
+
+// After a synchronisation: the persistent solve's error word is set when a wait between its
+// thread blocks ran out, which leaves the steps since the last check invalid.
+void check_wave_solve(rrg_ctx* c) {
+    if (!c->wave_solve_used || !c->wsync.p) return;
+    unsigned int e = 0;
+    RRG_CUDA(cudaMemcpyAsync(&e, c->wsync.as<char>() + kWaveSyncErrOffset, 4,
+                             cudaMemcpyDeviceToHost, c->stream));
+    RRG_CUDA(cudaStreamSynchronize(c->stream));
+    if (e != 0) {
+        RRG_CUDA(cudaMemsetAsync(c->wsync.p, 0, c->wsync.bytes, c->stream));
+        RRG_CUDA(cudaStreamSynchronize(c->stream));
+        throw Error(RRG_ERR_CUDA,
+                    "wave solve: a wait between thread blocks timed out; the state is invalid");
+    }
 }
 
 PmParticleArgs pm_args(rrg_ctx* c, int deposit_target) {
@@ -429,9 +466,11 @@ void record_wave_steps(rrg_ctx* c, int nsteps, bool prologue) {
         c->mg_cur = t;
     }
     for (int s = 0; s < nsteps; ++s) {
-        wave_source(c, true);
-        for (int k = 0; k < c->wave.iterations; ++k) wave_substep(c, w, nullptr);
-        gradient(c);
+        if (!solve_step_persistent(c, w, c->wave.iterations)) {
+            wave_source(c, true);
+            for (int k = 0; k < c->wave.iterations; ++k) wave_substep(c, w, nullptr);
+            gradient(c);
+        }
         if (s + 1 < nsteps) {
             const int t = 1 - c->mg_cur;
             PmParticleArgs a = pm_args(c, t);
@@ -585,7 +624,10 @@ RRG_API rrg_status rrg_set_stream(rrg_ctx* ctx, void* stream) {
 }
 
 RRG_API rrg_status rrg_synchronize(rrg_ctx* ctx) {
-    RRG_ENTRY(ctx, { RRG_CUDA(cudaStreamSynchronize(ctx->stream)); })
+    RRG_ENTRY(ctx, {
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_wave_solve(ctx);
+    })
 }
 
 RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos,
@@ -714,6 +756,7 @@ RRG_API rrg_status rrg_get_particles(rrg_ctx* ctx, double* pos, double* vel, dou
         if (grav)
             RRG_CUDA(cudaMemcpyAsync(grav, d + 9 * n, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
         RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_wave_solve(ctx);
     })
 }
 
@@ -746,8 +789,9 @@ RRG_API rrg_status rrg_init_grid(rrg_ctx* ctx, const rrg_grid_info* grid) {
         ctx->phi[1].alloc(nc * ctx->rsz);
         ctx->acc4.alloc(nc * v4b(ctx));
         ctx->maxbits.alloc(16);
+        ctx->wsync.alloc(wave_solve_sync_bytes(grid->nx));
         for (Buf* b : {&ctx->mg[0], &ctx->mg[1], &ctx->src, &ctx->phi[0], &ctx->phi[1],
-                       &ctx->acc4, &ctx->maxbits})
+                       &ctx->acc4, &ctx->maxbits, &ctx->wsync})
             RRG_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, ctx->stream));
         ctx->mg_cur = 0;
         ctx->phi_cur = 0;
@@ -939,6 +983,30 @@ RRG_API rrg_status rrg_solve_wave_equation(rrg_ctx* ctx, int max_iterations,
     })
 }
 
+RRG_API rrg_status rrg_solve_wave_and_field(rrg_ctx* ctx, int iterations) {
+    RRG_ENTRY(ctx, {
+        drop_pending(ctx);
+        require_grid(ctx);
+        RRG_REQUIRE(ctx->has_wave, RRG_ERR_STATE, "no wave parameters");
+        RRG_REQUIRE(iterations >= 1, RRG_ERR_INVALID, "iterations must be >= 1");
+        const WaveCoef w = wave_coef(ctx);
+        if (!solve_step_persistent(ctx, w, iterations)) {
+            if (ctx->src_dirty) wave_source(ctx, false);
+            for (int k = 0; k < iterations; ++k) wave_substep(ctx, w, nullptr);
+            gradient(ctx);
+        }
+    })
+}
+
+RRG_API rrg_status rrg_wave_solve_sync(rrg_ctx* ctx, void** dev_ptr, size_t* bytes) {
+    RRG_ENTRY(ctx, {
+        require_grid(ctx);
+        RRG_REQUIRE(dev_ptr && bytes, RRG_ERR_INVALID, "rrg_wave_solve_sync: NULL");
+        *dev_ptr = ctx->wsync.p;
+        *bytes = ctx->wsync.bytes;
+    })
+}
+
 RRG_API rrg_status rrg_calc_acceleration_field(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
         drop_pending(ctx);
@@ -974,6 +1042,7 @@ static void reduce_state(rrg_ctx* ctx, bool com) {
     RRG_CUDA(cudaMemcpyAsync(ctx->host_red, ctx->red_out.p, 12 * sizeof(double),
                              cudaMemcpyDeviceToHost, ctx->stream));
     RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+    check_wave_solve(ctx);
 }
 
 RRG_API rrg_status rrg_calc_conservation(rrg_ctx* ctx, rrg_conservation* out) {

@@ -1,4 +1,5 @@
-// Launchers of the sm_100a kernels (implemented in direct.cu, pm.cu, integrate.cu).
+// Launchers of the sm_100a kernels (implemented in direct.cu, pm.cu, wave_solve.cu,
+// integrate.cu).
 #pragma once
 
 #include "common.cuh"
@@ -110,6 +111,23 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
                       const WaveCoef& c, unsigned long long* maxbits, cudaStream_t s);
 // a = -grad phi on the grid (rm_p2mesh.cu:238-290): acc4[c] = (ax, ay, az, phi[c]).
 void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, cudaStream_t s);
+// One PM step's whole FP32 wave solve in one persistent cooperative kernel (wave_solve.cu):
+// source from the deposit mg (mg_zero cleared), `iterations` substeps over the levels phi0 /
+// phi1 (cur: which holds the current level; the result lands in phi[cur ^ (iterations & 1)],
+// the level before it in the other), then the gradient into acc4 (skipped when acc4 is null).
+// Periodic box without an absorbing layer only; the same results as launch_wave_source +
+// launch_wave_step + launch_gradient. sync: wave_solve_sync_bytes(nx) of device memory, zeroed
+// before the first use and kept between calls; its word at byte 65532 becomes non-zero when a
+// wait between blocks ran out (the step is then invalid and the memory must be zeroed again).
+// Returns false, launching nothing, where it does not apply (nx, residency,
+// RRG_WAVE_PERSIST=0).
+bool wave_solve_applicable(int nx);
+size_t wave_solve_sync_bytes(int nx);
+constexpr size_t kWaveSyncErrOffset = 65532;
+bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur,
+                       const unsigned long long* mg, unsigned long long* mg_zero, int shift_s,
+                       double dx, double rho_sub, const WaveCoef& w, float* src, float4* acc4,
+                       unsigned int* sync, size_t sync_bytes, cudaStream_t s);
 // Trilinear gather of acc4 to particles (rm_mesh2p.cu:48-114).
 void launch_interp(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
                    const void* acc4, void* acc, cudaStream_t s);

@@ -331,3 +331,111 @@ def test_step_by_step_calls_equal_one_long_call(prec, interval):
             np.testing.assert_array_equal(p[k], out[0][0][k])
         np.testing.assert_array_equal(gr["mass"], out[0][1]["mass"])
         np.testing.assert_array_equal(gr["grav"], out[0][1]["grav"])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+@pytest.mark.parametrize("nx,iterations", [(32, 20), (64, 7), (128, 20)])
+def test_persistent_wave_solve_equals_one_launch_per_substep(monkeypatch, prec, nx, iterations):
+    """Periodic FP32 grids of 32, 64 and 128 cells run each step's source, substeps and
+    gradient as one persistent kernel; RRG_WAVE_PERSIST=0 launches them one by one. Same bits
+    for the particles, the potential levels and the field, over steps with sorts in between,
+    an odd substep count (the level parity flips every step) and split calls."""
+    n, dt = 60000, 2e-3
+    pos, vel, m, s2 = disk(n, seed=nx + iterations)
+    g = _grid(nx)
+    vmax = np.max(np.linalg.norm(vel, axis=1))
+    wp = rg.WaveParams.make(g.dx, diss_base=1.0 / (4 * g.dx), wave_speed=10 * vmax,
+                            iterations=iterations, setup_iterations=100,
+                            steady_check_step=1000)
+    sim = rg.SimParams(time_max=1.0, dt_save=0.1, dt_dynamics=dt, saves_without_dump=2 ** 63,
+                       use_wave_model=1)
+    out, launches = [], []
+    for persist in ("1", "0"):
+        monkeypatch.setenv("RRG_WAVE_PERSIST", persist)
+        with _ctx(prec, pos, vel, m, s2, g) as c:
+            c.set_sort_interval(3)
+            c.set_wave_params(wp)
+            c.solver_init(sim)
+            c.precalc()
+            k0 = rg.kernel_launch_count()
+            c.calc_steps(4)
+            mid = c.get_particles()
+            c.calc_steps(5)
+            c.synchronize()
+            launches.append(rg.kernel_launch_count() - k0)
+            out.append((mid, c.get_particles(), c.get_grid(), c.get_wave_state()))
+    (mid1, p1, g1, w1), (mid0, p0, g0, w0) = out
+    for k in ("pos", "vel", "acc"):
+        np.testing.assert_array_equal(mid1[k], mid0[k])
+        np.testing.assert_array_equal(p1[k], p0[k])
+    for k in g1:
+        np.testing.assert_array_equal(g1[k], g0[k])
+    for a, b in zip(w1, w0):
+        np.testing.assert_array_equal(a, b)
+    # one kernel instead of source + substeps + gradient in each of the 9 steps
+    assert launches[0] + 9 * (iterations + 1) == launches[1]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+@pytest.mark.parametrize("nx", [64, 40])
+def test_solve_wave_and_field_equals_separate_calls(prec, nx):
+    """The one-call solve (the persistent kernel on FP32 / MIXED 64^3; separate launches on
+    40^3 and in FP64) leaves the same bits as solve_wave_equation + calc_acceleration_field."""
+    pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, prec)
+    wp.steady_check_step = 10 ** 6  # no steady checks inside the 7 substeps
+    out = []
+    for fused in (True, False):
+        with _ctx(prec, pos, vel, m, s2, g) as c:
+            c.set_wave_params(wp)
+            c.convert_particles_to_grid()
+            c.set_boundary_periodic(1.0)
+            c.set_grid_potential(phi0)
+            if fused:
+                c.solve_wave_and_field(7)
+            else:
+                it, _ = c.solve_wave_equation(7)
+                assert it == 7
+                c.calc_acceleration_field()
+            out.append((c.get_grid(), c.get_wave_state()))
+    (g1, w1), (g0, w0) = out
+    for k in g1:
+        np.testing.assert_array_equal(g1[k], g0[k])
+    for a, b in zip(w1, w0):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_persistent_solve_reports_a_wait_that_ran_out():
+    """Every wait between the persistent solve's thread blocks is bounded (~0.14 s). Rewinding
+    one block's epoch counter makes its neighbours wait for epochs it never publishes: the
+    waits run out, the kernel sets its error word and returns, the next synchronising call
+    raises, and after that the context computes the same bits as a fresh one."""
+    from cuda.bindings import runtime as cudart
+
+    nx = 64
+    pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, "fp32")
+
+    def fresh_solve(c):
+        c.set_wave_params(wp)
+        c.convert_particles_to_grid()
+        c.set_boundary_periodic(1.0)
+        c.set_grid_potential(phi0)
+        c.solve_wave_and_field(5)
+        return c.get_grid()
+
+    with _ctx("fp32", pos, vel, m, s2, g) as ref:
+        want = fresh_solve(ref)
+    with _ctx("fp32", pos, vel, m, s2, g) as c:
+        fresh_solve(c)
+        c.synchronize()
+        ptr, nbytes = c.wave_solve_sync()
+        assert ptr != 0 and nbytes >= 65536
+        zero = np.zeros(1, dtype=np.uint32)
+        err, = cudart.cudaMemcpy(ptr, zero.ctypes.data, 4, cudart.cudaMemcpyKind.cudaMemcpyHostToDevice)
+        assert err == cudart.cudaError_t.cudaSuccess
+        c.solve_wave_and_field(5)
+        with pytest.raises(rg.RRGError, match="timed out"):
+            c.synchronize()
+        # the sync memory is clear again and the context usable
+        got = fresh_solve(c)
+    for k in want:
+        np.testing.assert_array_equal(got[k], want[k])

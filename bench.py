@@ -233,6 +233,8 @@ def run_native(args):
     ctx.load_particles(pos, vel, mass, soft2)
     ctx.init_grid(grid)
     ctx.set_wave_params(wave)
+    if args.sort_interval is not None:
+        ctx.set_sort_interval(args.sort_interval)
     ctx.solver_init(sim)
     t0 = time.perf_counter()
     ctx.precalc()
@@ -315,6 +317,8 @@ def run_native(args):
            for k, v in dict(pos=pos, vel=vel, mass=mass, soft2=soft2).items()}
     ctx2.init_grid(grid)
     ctx2.set_wave_params(wave)
+    if args.sort_interval is not None:
+        ctx2.set_sort_interval(args.sort_interval)
     ctx2.load_particles(pin["pos"], pin["vel"], pin["mass"], pin["soft2"])
     ctx2.solver_init(sim)
     ctx2.precalc()
@@ -404,7 +408,9 @@ def run_native(args):
             "config": {"workload": WORKLOAD, "particles": N_PART, "grid": NX,
                        "substeps": SUBSTEPS, "dt": DT, "parallelism": f"replicas{world}",
                        "l2": "per-step working set ~140 MB > 126 MB L2; steps back to back",
-                       "setup_s": round(setup_s, 3)},
+                       "setup_s": round(setup_s, 3),
+                       "sort_interval": args.sort_interval if args.sort_interval is not None
+                       else "library default"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": k_e2e, "statistic": "median of 5 runs",
                     "runs": [N_PART * k_e2e * world / t for t in e2e_runs]},
@@ -435,6 +441,8 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sort-interval", type=int, default=None,
+                    help="steps between re-sorts of the particles by cell (default: the library's)")
     ap.add_argument("--setup-iterations", type=int, default=20000,
                     help="cap of the initial potential relaxation (profiling runs use fewer)")
     args = ap.parse_args()

@@ -133,7 +133,7 @@ struct rrg_ctx {
     rrg_sim_params sim{};
     double time = 0.0;
     uint64_t iter = 0;
-    int sort_interval = -1;          // -1: the strategy's default (64 steps in wave mode)
+    int sort_interval = -1;          // -1: the strategy's default (16 steps in wave mode)
     // Wave mode, between calc_steps calls: the last particle pass also predicted the next step,
     // so posm[1 - cur] (and poslo[1 - cur]) hold x_{n+1}, u its v + v*, and mg[1 - mg_cur] its
     // deposit. The synced state (x_n, v_n, a_n, deposit of x_n) is untouched; the next
@@ -401,10 +401,17 @@ void sort_particles(rrg_ctx* c) {
         c->id.alloc(4 * n);
         launch_iota(n, c->id.as<int32_t>(), c->stream);
     }
+    // with a pending prediction the predicted positions give the keys (they are deposited
+    // next), and the prediction is permuted with the synced state; its deposit grid is a sum
+    // over particles and does not depend on their order
+    const bool keep = c->pending;
+    const int other = 1 - c->cur;
+    const bool mixed = c->prec == RRG_PREC_MIXED;
     RRG_CUDA(cudaMemsetAsync(c->sort_counts.p, 0, c->sort_counts.bytes, c->stream));
     RRG_CUDA(cudaMemsetAsync(c->sort_cursor.p, 0, c->sort_cursor.bytes, c->stream));
-    launch_cell_keys(c->prec, n, c->P(), c->L(), c->gdev, c->sort_keys.as<uint32_t>(),
-                     c->sort_counts.as<uint32_t>(), c->stream);
+    launch_cell_keys(c->prec, n, keep ? c->posm[other].p : c->P(),
+                     mixed ? (keep ? c->poslo[other].p : c->L()) : nullptr, c->gdev,
+                     c->sort_keys.as<uint32_t>(), c->sort_counts.as<uint32_t>(), c->stream);
     launch_scan_counts(c->sort_counts.as<uint32_t>(), c->sort_offsets.as<uint32_t>(), nc,
                        c->sort_temp.p, c->sort_temp_bytes, c->stream);
     launch_sort_dest(n, c->sort_keys.as<uint32_t>(), c->sort_offsets.as<uint32_t>(),
@@ -416,7 +423,12 @@ void sort_particles(rrg_ctx* c) {
                                  c->stream));
     };
     permute(c->P(), v4b(c));
-    if (c->prec == RRG_PREC_MIXED) permute(c->L(), sizeof(V4<float>));
+    if (mixed) permute(c->L(), sizeof(V4<float>));
+    if (keep) {
+        permute(c->posm[other].p, v4b(c));
+        if (mixed) permute(c->poslo[other].p, sizeof(V4<float>));
+        permute(c->u.p, v4b(c));
+    }
     permute(c->vel.p, v4b(c));
     permute(c->acc.p, v4b(c));
     permute(c->pot.p, c->rsz);
@@ -1225,16 +1237,16 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
                 }
                 // long runs are recorded once per chunk length and replayed; in wave mode the
                 // particles are re-sorted by cell between chunks every sort_interval steps
+                // (16: particles drift about a tenth of a cell in 16 steps of the disk
+                // workload, and the deposit's warp aggregation degrades with the disorder)
                 const int interval =
-                    ctx->wave_mode ? (ctx->sort_interval < 0 ? 64 : ctx->sort_interval) : 0;
+                    ctx->wave_mode ? (ctx->sort_interval < 0 ? 16 : ctx->sort_interval) : 0;
                 int left = nsteps;
                 while (left > 0) {
                     int chunk = std::min(left, 64);
                     if (interval > 0) {
-                        if (ctx->steps_since_sort >= interval) {
-                            drop_pending(ctx);  // the sort permutes the synced state only
-                            sort_particles(ctx);
-                        }
+                        if (ctx->steps_since_sort >= interval)
+                            sort_particles(ctx);  // (a pending prediction is permuted along)
                         chunk = static_cast<int>(
                             std::min<int64_t>(chunk, interval - ctx->steps_since_sort));
                     }

@@ -57,10 +57,14 @@ __device__ __forceinline__ void cic_axis(double x, double dmin, double inv_dx, i
 }
 
 // Deposits one particle (all lanes of the warp call this together, converged).
-// Lanes with the same base cell form a group (__match_any_sync); each of the 8 corner values
-// is summed over the group with one redux.sync and added by the group leader with one 64-bit
-// atomic. Values fit in 27 bits (the scale S is chosen so that m_max 2^S <= 2^26), so a warp
-// sum fits the 32-bit redux.
+// Consecutive lanes with the same base cell form a run (particles sorted by cell make long
+// runs); each of the 8 corner values is summed over the run by a segmented warp scan (five
+// full-warp shuffles, no divergent masks) and the run's last lane adds the eight sums with
+// 64-bit atomics. Values fit in 27 bits (the scale S is chosen so that m_max 2^S <= 2^26), so a
+// warp's sum fits 32 bits; integer sums are exact in any order, so the grid does not depend on
+// how particles fall into runs. (Grouping lanes with __match_any_sync and summing each group
+// with __reduce_add_sync cost twice as much: every distinct group mask in a warp is a separate
+// divergent pass.)
 __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y, double z,
                                                  double m, const GridDev& g, double scale,
                                                  unsigned long long* __restrict__ grid) {
@@ -72,10 +76,16 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
         cic_axis(y, g.domain_min, g.inv_dx, nx, j0, j1, wy0, wy1);
         cic_axis(z, g.domain_min, g.inv_dx, nx, k0, k1, wz0, wz1);
     }
-    const int64_t nx2 = static_cast<int64_t>(nx) * nx;
-    const int base = active ? (i0 + j0 * nx + k0 * static_cast<int>(nx2)) : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, base);
-    const bool leader = (threadIdx.x & 31) == (__ffs(peers) - 1);
+    const int nx2 = nx * nx;  // nx^3 < 2^31 (nx <= 1024)
+    const int base = active ? (i0 + j0 * nx + k0 * nx2) : -1;
+    const int lane = threadIdx.x & 31;
+    // every lane takes part in every shuffle (none behind a short-circuit or a branch)
+    const int below = __shfl_up_sync(0xffffffffu, base, 1);
+    const int above = __shfl_down_sync(0xffffffffu, base, 1);
+    const bool head = lane == 0 || below != base;
+    const bool tail = lane == 31 || above != base;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // this run's first lane
     const double ms = __dmul_rn(m, scale);
     // corner order and weight products as rm_p2mesh.cu:219-235
     const int ii[8] = {i0, i1, i0, i1, i0, i1, i0, i1};
@@ -85,21 +95,24 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
     unsigned sum[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        unsigned q = 0;
+        unsigned v = 0;
         if (active) {
             const double w = __dmul_rn(__dmul_rn(wxs[c & 1], wys[(c >> 1) & 1]), wzs[c >> 2]);
-            q = static_cast<unsigned>(__double2ll_rn(__dmul_rn(ms, w)));
+            v = static_cast<unsigned>(__double2ll_rn(__dmul_rn(ms, w)));
         }
-        sum[c] = __reduce_add_sync(peers, q);
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane - d >= first) v += t;
+        }
+        sum[c] = v;  // at the run's last lane: the run's total
     }
-    // one divergent branch: the group leader adds the eight corner sums
-    if (active && leader) {
+    if (active && tail) {
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            if (sum[c] != 0u) {
-                const int64_t a = ii[c] + static_cast<int64_t>(jj[c]) * nx + kk[c] * nx2;
-                atomicAdd(grid + a, static_cast<unsigned long long>(sum[c]));
-            }
+            if (sum[c] != 0u)
+                atomicAdd(grid + (kk[c] * nx + jj[c]) * nx + ii[c],
+                          static_cast<unsigned long long>(sum[c]));
         }
     }
 }

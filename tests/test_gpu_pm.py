@@ -217,9 +217,11 @@ def test_pm_steps_match_oracle(prec):
     assert np.median(rel_err(got["acc"], ra)) <= tol_a
 
 
-def test_sorting_by_cell_changes_nothing_but_memory_order():
-    """The counting sort between fused chunks permutes memory only: results are bit-identical
-    with and without it, and particles come back in their original order."""
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_sorting_by_cell_changes_nothing_but_memory_order(prec):
+    """The counting sort between fused chunks permutes memory only (the synced state and a
+    pending prediction alike): results are bit-identical with and without it, and particles
+    come back in their original order."""
     nx, n, dt = 32, 30000, 2e-3
     pos, vel, m, s2 = disk(n, seed=2)
     g = _grid(nx)
@@ -230,7 +232,7 @@ def test_sorting_by_cell_changes_nothing_but_memory_order():
                        use_wave_model=1)
     out = []
     for interval in (0, 7):
-        with _ctx("fp32", pos, vel, m, s2, g) as c:
+        with _ctx(prec, pos, vel, m, s2, g) as c:
             c.set_sort_interval(interval)
             c.set_wave_params(wp)
             c.solver_init(sim)

@@ -327,10 +327,10 @@ def run_native(args):
     ctx2.synchronize()
     # each step's diagnostics come down into pinned host memory asynchronously; the host reads
     # step k's while steps k + 1 .. k + DEPTH - 1 are queued (DEPTH slots, one CUDA event
-    # each), so a late host thread does not stall the GPU. The whole leg runs five times and
-    # the median counts: it is timed on the host clock, which a shared host's scheduling can
-    # stretch now and then.
-    depth = 3
+    # each: ~2 ms of GPU work), so a host thread that the shared host deschedules for a moment
+    # does not stall the GPU. The whole leg runs five times and the median counts: it is timed
+    # on the host clock.
+    depth = 16
     sums = torch.zeros((depth, 12), dtype=torch.float64).pin_memory().numpy()
     done = [torch.cuda.Event() for _ in range(depth)]
     e2e_runs = []

@@ -113,6 +113,7 @@ struct rrg_ctx {
     int mg_cur = 0;
     int phi_cur = 0;
     bool src_dirty = true;
+    bool src_valid = true;           // false: the fused steps left the source grid unwritten
     int shift_s = 0;
     bool has_wave = false;
     rrg_wave_params wave{};
@@ -248,6 +249,7 @@ void wave_source(rrg_ctx* c, bool zero_other) {
                                  c->stream));
     }
     c->src_dirty = false;
+    c->src_valid = true;
 }
 
 void wave_substep(rrg_ctx* c, const WaveCoef& w, unsigned long long* maxbits) {
@@ -263,18 +265,21 @@ void gradient(rrg_ctx* c) {
 // The source, `iterations` substeps and the gradient as the persistent kernel, where it applies
 // (FP32 grids, periodic box without an absorbing layer, a grid whose blocks all fit on the GPU
 // at once). The results equal those of wave_source + wave_substep x iterations + gradient;
-// false: nothing launched, the caller launches those.
-bool solve_step_persistent(rrg_ctx* c, const WaveCoef& w, int iterations) {
+// false: nothing launched, the caller launches those. store_src = false leaves the source grid
+// unwritten (marked stale): the fused steps never read it.
+bool solve_step_persistent(rrg_ctx* c, const WaveCoef& w, int iterations, bool store_src) {
     if (c->prec == RRG_PREC_FP64 || c->bc_type != RRG_BC_PERIODIC || c->keep_layer) return false;
     if (!launch_wave_solve(c->grid.nx, iterations, c->phi[0].as<float>(),
                            c->phi[1].as<float>(), c->phi_cur,
                            c->mg[c->mg_cur].as<unsigned long long>(),
                            c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
-                           c->rho_mean, w, c->src.as<float>(), c->acc4.as<float4>(),
+                           c->rho_mean, w, store_src ? c->src.as<float>() : nullptr,
+                           c->acc4.as<float4>(),
                            c->wsync.as<unsigned int>(), c->wsync.bytes, c->stream))
         return false;
     if (iterations % 2 == 1) c->phi_cur = 1 - c->phi_cur;
     c->src_dirty = false;
+    c->src_valid = store_src;
     c->wave_solve_used = true;
     return true;
 }
@@ -320,7 +325,7 @@ int solve_wave(rrg_ctx* c, int max_iterations, double* last_rel) {
     RRG_REQUIRE(max_iterations >= 0, RRG_ERR_INVALID, "max_iterations must be >= 0");
     RRG_REQUIRE(c->wave.steady_check_step > 0, RRG_ERR_INVALID,
                 "steady_check_step must be positive (used as a modulus, wave.cu:275)");
-    if (c->src_dirty) wave_source(c, false);
+    if (c->src_dirty || !c->src_valid) wave_source(c, false);
     const WaveCoef w = wave_coef(c);
     int hold = 0;
     double rel = -1.0;
@@ -478,7 +483,7 @@ void record_wave_steps(rrg_ctx* c, int nsteps, bool prologue) {
         c->mg_cur = t;
     }
     for (int s = 0; s < nsteps; ++s) {
-        if (!solve_step_persistent(c, w, c->wave.iterations)) {
+        if (!solve_step_persistent(c, w, c->wave.iterations, false)) {
             wave_source(c, true);
             for (int k = 0; k < c->wave.iterations; ++k) wave_substep(c, w, nullptr);
             gradient(c);
@@ -1002,8 +1007,8 @@ RRG_API rrg_status rrg_solve_wave_and_field(rrg_ctx* ctx, int iterations) {
         RRG_REQUIRE(ctx->has_wave, RRG_ERR_STATE, "no wave parameters");
         RRG_REQUIRE(iterations >= 1, RRG_ERR_INVALID, "iterations must be >= 1");
         const WaveCoef w = wave_coef(ctx);
-        if (!solve_step_persistent(ctx, w, iterations)) {
-            if (ctx->src_dirty) wave_source(ctx, false);
+        if (!solve_step_persistent(ctx, w, iterations, true)) {
+            if (ctx->src_dirty || !ctx->src_valid) wave_source(ctx, false);
             for (int k = 0; k < iterations; ++k) wave_substep(ctx, w, nullptr);
             gradient(ctx);
         }

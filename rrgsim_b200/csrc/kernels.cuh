@@ -114,7 +114,8 @@ void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, c
 // One PM step's whole FP32 wave solve in one persistent cooperative kernel (wave_solve.cu):
 // source from the deposit mg (mg_zero cleared), `iterations` substeps over the levels phi0 /
 // phi1 (cur: which holds the current level; the result lands in phi[cur ^ (iterations & 1)],
-// the level before it in the other), then the gradient into acc4 (skipped when acc4 is null).
+// the level before it in the other), then the gradient into acc4 (skipped when acc4 is null);
+// the source is also stored to src unless src is null.
 // Periodic box without an absorbing layer only; the same results as launch_wave_source +
 // launch_wave_step + launch_gradient. sync: wave_solve_sync_bytes(nx) of device memory, zeroed
 // before the first use and kept between calls; its word at byte 65532 becomes non-zero when a

@@ -92,7 +92,7 @@ struct SolveArgs {
     unsigned long long* mg_zero;    // the other deposit grid: cleared
     double inv_scale, inv_dx3, rho_sub;
     float km, ka, ko, kf, grad_coef;
-    float* src;                     // the source is also stored (other paths read it)
+    float* src;                     // nullptr, or where the source is also stored
     float4* acc4;                   // nullptr: no gradient
     unsigned int* sync;             // sync_bytes_for(blocks), zeroed before the first launch
 };
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
             }
             const float4 s4 = make_float4(sv[0], sv[1], sv[2], sv[3]);
             srcs[k * kThreads + tid] = s4;
-            __stcg(reinterpret_cast<float4*>(a.src) + o4, s4);
+            if (a.src != nullptr) __stcg(reinterpret_cast<float4*>(a.src) + o4, s4);
             const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
             __stcg(z2 + 2 * o4, zz);
             __stcg(z2 + 2 * o4 + 1, zz);

@@ -1,4 +1,6 @@
 // Leapfrog (predict/correct), FP64 diagnostics and state packing on sm_100a.
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace rrg {
@@ -143,37 +145,50 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
             casc_add(acc[11], m * z);
         }
     }
-    __shared__ DD s[kRedThreads / 32][kRedVals];
+    // block partials: every thread's sums go to shared memory, then warp w reduces values
+    // w, w + 8, ...: each lane adds 8 threads' sums in order, then a fixed shuffle tree (about
+    // a third of the FP64 work of a shuffle tree per value in every warp)
+    __shared__ DD red[NV][kRedThreads];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        const DD t = warp_sum_dd(dd_norm(acc[k].s, acc[k].c));
-        if (lane == 0) s[w][k] = t;
-    }
+    for (int k = 0; k < NV; ++k) red[k][threadIdx.x] = dd_norm(acc[k].s, acc[k].c);
     __syncthreads();
-    if (threadIdx.x < kRedVals) {
+    for (int k = w; k < kRedVals; k += kRedThreads / 32) {
         DD t{0.0, 0.0};
-        if (threadIdx.x < NV)
-            for (int ww = 0; ww < kRedThreads / 32; ++ww) t = dd_add(t, s[ww][threadIdx.x]);
-        const int64_t o = (static_cast<int64_t>(blockIdx.x) * kRedVals + threadIdx.x) * 2;
-        partial[o] = t.hi;
-        partial[o + 1] = t.lo;
+        if (k < NV) {
+#pragma unroll
+            for (int j = lane; j < kRedThreads; j += 32) t = dd_add(t, red[k][j]);
+            t = warp_sum_dd(t);
+        }
+        if (lane == 0) {
+            const int64_t o = (static_cast<int64_t>(blockIdx.x) * kRedVals + k) * 2;
+            partial[o] = t.hi;
+            partial[o + 1] = t.lo;
+        }
     }
 }
 
-// One warp per reduced value: lane l sums blocks l, l + 32, ... in order, then a fixed
-// shuffle tree, all in double-double; the result is its rounded high part.
-__global__ void conservation_finish(const double* __restrict__ partial, int nblocks,
-                                    double* __restrict__ out) {
-    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (k >= kRedVals) return;
+// One block per reduced value: thread t sums block partials t, t + 256, ... in order, then a
+// fixed shuffle tree per warp and the warps in order, all in double-double; the result is its
+// rounded high part. (Summing in the last block of the main kernel instead, with the other
+// blocks counted by an atomic, measured slower: one block then does twelve blocks' work.)
+__global__ void __launch_bounds__(kRedThreads) conservation_finish(
+    const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+    const int k = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     DD t{0.0, 0.0};
-    for (int b = lane; b < nblocks; b += 32) {
+    for (int b = threadIdx.x; b < nblocks; b += kRedThreads) {
         const int64_t o = (static_cast<int64_t>(b) * kRedVals + k) * 2;
         t = dd_add(t, DD{partial[o], partial[o + 1]});
     }
     t = warp_sum_dd(t);
-    if (lane == 0) out[k] = t.hi;
+    __shared__ DD s[kRedThreads / 32];
+    if (lane == 0) s[w] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD r{0.0, 0.0};
+        for (int ww = 0; ww < kRedThreads / 32; ++ww) r = dd_add(r, s[ww]);
+        out[k] = r.hi;
+    }
 }
 
 // Host FP64 AoS -> device state.
@@ -275,9 +290,17 @@ void launch_correct(int prec, int64_t n, void* vel, const void* acc, const void*
 }
 
 // Two blocks per SM: the sums are FP64-bound, and few partials keep the final pass short.
+// RRG_CONS_BLOCKS caps the block count (for sweeps; the partial buffer is sized from this).
+// 592 (4 per SM) measured best at 2^20 particles: 296 left the FP64 chains latency-bound,
+// more blocks cost more in the per-block epilogue than they gain.
 int conservation_blocks(int64_t n) {
+    static const int cap = [] {
+        const char* e = std::getenv("RRG_CONS_BLOCKS");
+        const int v = e ? std::atoi(e) : 0;
+        return v > 0 ? v : 592;
+    }();
     const int b = div_up(n, kRedThreads);
-    return b < 296 ? (b < 1 ? 1 : b) : 296;
+    return b < cap ? (b < 1 ? 1 : b) : cap;
 }
 
 void launch_conservation(int prec, int64_t n, const void* posm, const void* poslo,
@@ -300,7 +323,7 @@ void launch_conservation(int prec, int64_t n, const void* posm, const void* posl
     }
 #undef RRG_CONS
     RRG_LAUNCHED();
-    conservation_finish<<<1, 32 * kRedVals, 0, s>>>(partial, nblocks, out);
+    conservation_finish<<<kRedVals, kRedThreads, 0, s>>>(partial, nblocks, out);
     RRG_LAUNCHED();
 }
 

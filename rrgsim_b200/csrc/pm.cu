@@ -98,7 +98,11 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
         unsigned v = 0;
         if (active) {
             const double w = __dmul_rn(__dmul_rn(wxs[c & 1], wys[(c >> 1) & 1]), wzs[c >> 2]);
-            v = static_cast<unsigned>(__double2ll_rn(__dmul_rn(ms, w)));
+            // round to the nearest integer, ties to even, as __double2ll_rn: adding 1.5 * 2^52
+            // leaves the integer in the low mantissa bits (exact for 0 <= value < 2^31; values
+            // here are below 2^27), an FP64 add instead of a conversion on the XU pipe
+            v = static_cast<unsigned>(
+                __double2loint(__dadd_rn(__dmul_rn(ms, w), 6755399441055744.0)));
         }
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -756,7 +760,7 @@ __global__ void __launch_bounds__(256) ngp_project_kernel(int64_t n, const void*
 //                                                                             deposit)
 // ----------------------------------------------------------------------------------------------
 template <typename R, bool MIXED, int MODE>
-__global__ void __launch_bounds__(256) pm_particle_kernel(PmParticleArgs a, double scale) {
+__global__ void __launch_bounds__(256, 6) pm_particle_kernel(PmParticleArgs a, double scale) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool active = i < a.n;
     V4<R>* posm = static_cast<V4<R>*>(a.posm);

@@ -407,8 +407,8 @@ void sort_particles(rrg_ctx* c) {
         launch_iota(n, c->id.as<int32_t>(), c->stream);
     }
     // with a pending prediction the predicted positions give the keys (they are deposited
-    // next), and the prediction is permuted with the synced state; its deposit grid is a sum
-    // over particles and does not depend on their order
+    // next) and the prediction is permuted; its deposit grid is a sum over particles and does
+    // not depend on their order
     const bool keep = c->pending;
     const int other = 1 - c->cur;
     const bool mixed = c->prec == RRG_PREC_MIXED;
@@ -427,15 +427,19 @@ void sort_particles(rrg_ctx* c) {
         RRG_CUDA(cudaMemcpyAsync(arr, c->sort_stage.p, elem * n, cudaMemcpyDeviceToDevice,
                                  c->stream));
     };
-    permute(c->P(), v4b(c));
-    if (mixed) permute(c->L(), sizeof(V4<float>));
     if (keep) {
+        // the prediction and its u; the synced positions, velocities and accelerations are
+        // not read again: the sort is always followed by a chunk that adopts the prediction,
+        // and its last pass rewrites all three before the call returns
         permute(c->posm[other].p, v4b(c));
         if (mixed) permute(c->poslo[other].p, sizeof(V4<float>));
         permute(c->u.p, v4b(c));
+    } else {
+        permute(c->P(), v4b(c));
+        if (mixed) permute(c->L(), sizeof(V4<float>));
+        permute(c->vel.p, v4b(c));
+        permute(c->acc.p, v4b(c));
     }
-    permute(c->vel.p, v4b(c));
-    permute(c->acc.p, v4b(c));
     permute(c->pot.p, c->rsz);
     if (!c->soft_uniform) permute(c->hsoft.p, c->rsz);
     permute(c->id.p, 4);

@@ -336,12 +336,13 @@ def test_step_by_step_calls_equal_one_long_call(prec, interval):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
-@pytest.mark.parametrize("nx,iterations", [(32, 20), (64, 7), (128, 20)])
+@pytest.mark.parametrize("nx,iterations", [(32, 20), (64, 7), (64, 1), (128, 20)])
 def test_persistent_wave_solve_equals_one_launch_per_substep(monkeypatch, prec, nx, iterations):
     """Periodic FP32 grids of 32, 64 and 128 cells run each step's source, substeps and
     gradient as one persistent kernel; RRG_WAVE_PERSIST=0 launches them one by one. Same bits
     for the particles, the potential levels and the field, over steps with sorts in between,
-    an odd substep count (the level parity flips every step) and split calls."""
+    odd substep counts (the level parity flips every step; one substep swaps the final and the
+    previous level within the launch) and split calls."""
     n, dt = 60000, 2e-3
     pos, vel, m, s2 = disk(n, seed=nx + iterations)
     g = _grid(nx)

@@ -303,7 +303,7 @@ RRG_API rrg_status rrg_set_wave_state(rrg_ctx* ctx, const double* phi_cur,
 
 /* Sorts particles by grid cell (counting sort) so deposits from one warp hit few cells.
  * Host-visible order is unchanged (rrg_get_particles undoes the permutation). The wave
- * strategy re-sorts on its own every `interval` steps (default 16); 0 disables it. Results do
+ * strategy re-sorts on its own every `interval` steps (default 64); 0 disables it. Results do
  * not depend on the interval. */
 RRG_API rrg_status rrg_set_sort_interval(rrg_ctx* ctx, int interval);
 

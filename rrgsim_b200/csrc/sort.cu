@@ -2,7 +2,7 @@
 //
 // Particles that share a base cell deposit into the same eight grid cells and gather from the
 // same eight field cells. Stored next to each other, one warp's deposits collapse into a few
-// atomics (cic_deposit_warp groups lanes by base cell) and its gathers hit the same cache
+// atomics (cic_deposit_warp sums runs of equal cells) and its gathers hit the same cache
 // lines. The sort is a counting sort: cell keys + histogram, an exclusive scan of the counts,
 // a destination per particle, then one scatter per particle array. Results do not depend on
 // the order (the deposit is integer, everything else is per particle); only memory order

@@ -65,6 +65,36 @@ def test_cic_run_to_run_deterministic():
     np.testing.assert_array_equal(grids[0], grids[1])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+def test_cic_same_grid_in_any_particle_order(prec):
+    """The deposit sums runs of equal cells per warp, sorting a warp's cells first when they
+    interleave: particles sorted by cell (few runs per warp), sorted then moved a little (runs
+    broken up), and shuffled (a warp sort in nearly every warp) give the same fixed-point grid,
+    the oracle's."""
+    rng = np.random.default_rng(17)
+    pos, vel, m, s2 = disk(200000, seed=17)
+    g = _grid(64)
+    key = np.floor((pos + 8.0) / g.dx - 0.5).clip(0, 63).astype(np.int64)
+    order = np.argsort((key[:, 2] * 64 + key[:, 1]) * 64 + key[:, 0], kind="stable")
+    moved = pos[order] + 0.3 * g.dx * rng.uniform(-1, 1, (len(pos), 3))
+    shuffled = rng.permutation(len(pos))
+    cases = [(pos[order], m[order]), (moved, m[order]), (pos[shuffled], m[shuffled]),
+             (moved[::-1].copy(), m[order][::-1].copy())]
+    grids = []
+    for p, mm in cases:
+        with _ctx(prec, p, vel[: len(p)], mm, s2, g) as c:
+            c.convert_particles_to_grid()
+            grids.append(c.get_grid()["mass"])
+            shift = c.deposit_scale()
+    np.testing.assert_array_equal(grids[0], grids[2])
+    np.testing.assert_array_equal(grids[1], grids[3])
+    held = (lambda a: a) if prec == "mixed" else f32
+    og = _orc_grid(g)
+    for (p, mm), got in zip(cases[:2], grids[:2]):
+        q = orc.cic_fixed(held(p), f32(mm), og, shift)
+        np.testing.assert_array_equal(got, q.astype(np.float64) * 2.0 ** -shift)
+
+
 def _wave_setup(nx, prec, seed=11):
     rng = np.random.default_rng(seed)
     pos, vel, m, s2 = disk(20000, seed=seed)

@@ -65,7 +65,7 @@ def test_cic_run_to_run_deterministic():
     np.testing.assert_array_equal(grids[0], grids[1])
 
 
-@pytest.mark.parametrize("prec", ["fp32", "mixed"])
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
 def test_cic_same_grid_in_any_particle_order(prec):
     """The deposit sums runs of equal cells per warp, sorting a warp's cells first when they
     interleave: particles sorted by cell (few runs per warp), sorted then moved a little (runs
@@ -88,10 +88,11 @@ def test_cic_same_grid_in_any_particle_order(prec):
             shift = c.deposit_scale()
     np.testing.assert_array_equal(grids[0], grids[2])
     np.testing.assert_array_equal(grids[1], grids[3])
-    held = (lambda a: a) if prec == "mixed" else f32
+    held_pos = (lambda a: a) if prec != "fp32" else f32
+    held_m = (lambda a: a) if prec == "fp64" else f32
     og = _orc_grid(g)
     for (p, mm), got in zip(cases[:2], grids[:2]):
-        q = orc.cic_fixed(held(p), f32(mm), og, shift)
+        q = orc.cic_fixed(held_pos(p), held_m(mm), og, shift)
         np.testing.assert_array_equal(got, q.astype(np.float64) * 2.0 ** -shift)
 
 

@@ -101,6 +101,22 @@ def main():
     wave = [1.0 / (4 * dx), 0.01, c, 3000, 20, 1e-5, 500, 10, 3]
     pm_case(L, "ref_pm_disk2048_nx32_steady", pos, vel, np.full(n, 1.0 / n),
             np.full(n, 1e-4), nx, dx, 0.2, wave, 2e-3, 3, out)
+
+    # 5. a larger disk on a 32^3 grid without a steady check inside the step (the fused steps'
+    # whole per-step solve), and 6. on a 64^3 grid with an odd substep count
+    n = 8192
+    pos, vel = rg.generate_exp_disk(2, n, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1, 0.0, 0.0)
+    c = 10.0 * float(np.max(np.linalg.norm(vel, axis=1)))
+    nx = 32
+    dx = 16.0 / nx
+    wave = [1.0 / (4 * dx), 0.0, c, 1000, 20, 1e-6, 5000, 1000, 3]
+    pm_case(L, "ref_pm_disk8192_nx32", pos, vel, np.full(n, 1.0 / n), np.full(n, 1e-4), nx, dx,
+            0.2, wave, 2e-3, 6, out)
+    nx = 64
+    dx = 16.0 / nx
+    wave = [1.0 / (4 * dx), 0.0, c, 1000, 7, 1e-6, 5000, 1000, 3]
+    pm_case(L, "ref_pm_disk8192_nx64_odd", pos, vel, np.full(n, 1.0 / n), np.full(n, 1e-4), nx,
+            dx, 0.2, wave, 2e-3, 5, out)
     for f in sorted(out.glob("ref_*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -85,6 +85,11 @@ def main():
     soft2 = np.concatenate([np.full(256, 0.004 ** 2), np.full(256, 0.05 ** 2)])
     nbody_case(L, "ref_nbody_two_components512", pos, vel, mass, soft2, 1e-3, 10, out)
 
+    # 2b. the Plummer configuration at N = 4096 (eps = 0.01, dt = 1e-3), 20 steps
+    pos, vel = rg.generate_plummer(0, 4096, 1.0, 1.0, 20.0)
+    nbody_case(L, "ref_nbody_plummer4096", pos, vel, np.full(4096, 1 / 4096),
+               np.full(4096, 1e-4), 1e-3, 20, out)
+
     # 3. exponential disk on a 16^3 periodic wave grid spanning +-8 (dx = 1)
     n, nx = 2048, 16
     pos, vel = rg.generate_exp_disk(1, n, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1, 0.0, 0.0)

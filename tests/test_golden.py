@@ -13,7 +13,7 @@ import rrgsim_b200 as rg
 from helpers import rel_err
 
 GOLD = Path(__file__).resolve().parent / "golden"
-NBODY = ["ref_nbody_plummer512", "ref_nbody_two_components512"]
+NBODY = ["ref_nbody_plummer512", "ref_nbody_two_components512", "ref_nbody_plummer4096"]
 # the last two run through the fused steps' persistent wave solve in FP32 (periodic, 32^3 and
 # 64^3, no steady check inside a step)
 PM = ["ref_pm_disk2048_nx16", "ref_pm_disk2048_nx32_steady", "ref_pm_disk8192_nx32",

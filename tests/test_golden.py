@@ -14,8 +14,8 @@ from helpers import rel_err
 
 GOLD = Path(__file__).resolve().parent / "golden"
 NBODY = ["ref_nbody_plummer512", "ref_nbody_two_components512", "ref_nbody_plummer4096"]
-# the last two run through the fused steps' persistent wave solve in FP32 (periodic, 32^3 and
-# 64^3, no steady check inside a step)
+# the last two run through the fused steps' persistent wave solve in FP32 and MIXED (periodic,
+# 32^3 and 64^3, no steady check inside a step)
 PM = ["ref_pm_disk2048_nx16", "ref_pm_disk2048_nx32_steady", "ref_pm_disk8192_nx32",
       "ref_pm_disk8192_nx64_odd"]
 
@@ -109,7 +109,7 @@ def test_gpu_nbody_matches_reference(name, prec):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
 @pytest.mark.parametrize("name", PM)
 def test_gpu_pm_matches_reference(name, prec):
     g = load(name)

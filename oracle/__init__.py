@@ -126,6 +126,8 @@ def ref_lib():
                             dp]
     L.ref_pm.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_int, C.c_double, C.c_double, dp,
                          C.c_double, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp]
+    L.ref_wave_bc.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_int, C.c_double, C.c_double, dp,
+                              C.c_int, C.c_double, dp, dp, C.c_int, dp, dp]
     return L
 
 

@@ -195,4 +195,60 @@ int ref_pm(int64_t n, const double* pos, const double* vel, const double* mass,
     }
 }
 
+// The reference's wave solver under a non-periodic or layered boundary (wave.cu:18-104, set up
+// by set_boundary_monopole / set_boundary_periodic, :196-228), which its precalc leaves
+// commented out (rrgsim_integration_rect.cuh:57-64): CIC of the particles, the boundary
+// (bc = 0: periodic keeping the absorbing layer, 1: monopole Dirichlet, 2: monopole radiative,
+// with total_mass and com), both potential levels set to phi_init, then `iterations` substeps
+// with no steady check. wave[] as for ref_pm. Outputs: mass (nx^3) and the final potential.
+int ref_wave_bc(int64_t n, const double* pos, const double* vel, const double* mass,
+                const double* soft2, int nx, double dx, double bc_frac, const double* wave,
+                int bc, double total_mass, const double* com, const double* phi_init,
+                int iterations, double* mass_out, double* phi_out) {
+    try {
+        auto pd = make_particles(n, pos, vel, mass, soft2);
+        auto pctx = rrgsim::common::initialize_particles_context_(pd);
+        auto grid = make_grid(nx, dx, bc_frac);
+        auto gctx = rrgsim::common::initialize_grid_context_(grid);
+        rrgsim::common::WaveParams wp{};
+        wp.diss_base = wave[0];
+        wp.diss_extra = wave[1];
+        wp.wave_speed = wave[2];
+        wp.setup_iterations = static_cast<int>(wave[3]);
+        wp.iterations = static_cast<int>(wave[4]);
+        wp.tolerance = wave[5];
+        wp.print_step = static_cast<int>(wave[6]);
+        wp.steady_check_step = static_cast<int>(wave[7]);
+        wp.steady_hold_steps = static_cast<int>(wave[8]);
+        wp.dt = 0.5 * dx / (wp.wave_speed * std::sqrt(3.0));  // io_json.cpp:178
+        // grid_info_ came with the grid context; the wave parameters as the strategy's init
+        // uploads them (rrgsim_integration_rect.cuh:35-40)
+        RR::CUDA::CuCopyToSymbol(wp, rrgsim::common::wave_params_, RR::CUDA::ToDevice);
+        rrgsim::rect_mesh::convert_particles_to_grid(pctx, gctx);
+        if (bc == 0)
+            rrgsim::wave::set_boundary_periodic(total_mass, grid, true);
+        else
+            rrgsim::wave::set_boundary_monopole(total_mass, make_double3(com[0], com[1], com[2]),
+                                                bc == 2, dx);
+        const size_t nc = static_cast<size_t>(nx) * nx * nx;
+        std::vector<double> phi(phi_init, phi_init + nc);
+        gctx->grav_prev_ = phi;
+        gctx->grav_curr_ = phi;
+        rrgsim::wave::solve_wave_equation(gctx, wp, iterations);
+        if (mass_out) {
+            auto m = gctx->mass_.to_vector();
+            std::memcpy(mass_out, m.data(), sizeof(double) * nc);
+        }
+        if (phi_out) {
+            auto p = gctx->grav_curr_.to_vector();
+            std::memcpy(phi_out, p.data(), sizeof(double) * nc);
+        }
+        RR::CUDA::check(cudaGetLastError(), "ref_wave_bc");
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 }  // extern "C"

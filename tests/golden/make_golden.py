@@ -66,6 +66,22 @@ def pm_case(L, name, pos, vel, mass, soft2, nx, dx, bc_frac, wave, dt, steps, ou
                         phi_n=phi_n)
 
 
+def wave_bc_case(L, name, pos, vel, mass, soft2, nx, dx, bc_frac, wave, bc, total_mass, com,
+                 phi_init, iterations, out: Path):
+    n = len(mass)
+    nc = nx ** 3
+    mass0, phi = np.empty(nc), np.empty(nc)
+    w = np.asarray(wave, dtype=np.float64)
+    com = np.asarray(com, dtype=np.float64)
+    rc = L.ref_wave_bc(n, _p(pos), _p(vel), _p(mass), _p(soft2), nx, dx, bc_frac, _p(w), bc,
+                       total_mass, _p(com), _p(phi_init), iterations, _p(mass0), _p(phi))
+    if rc:
+        raise RuntimeError(L.ref_last_error().decode())
+    np.savez_compressed(out / f"{name}.npz", pos=pos, vel=vel, mass=mass, soft2=soft2, nx=nx,
+                        dx=dx, bc_frac=bc_frac, wave=w, bc=bc, total_mass=total_mass, com=com,
+                        phi_init=phi_init, iterations=iterations, mass0=mass0, phi=phi)
+
+
 def main():
     out = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent
     out.mkdir(parents=True, exist_ok=True)
@@ -122,6 +138,18 @@ def main():
     wave = [1.0 / (4 * dx), 0.0, c, 1000, 7, 1e-6, 5000, 1000, 3]
     pm_case(L, "ref_pm_disk8192_nx64_odd", pos, vel, np.full(n, 1.0 / n), np.full(n, 1e-4), nx,
             dx, 0.2, wave, 2e-3, 5, out)
+    # 7. the reference's other boundaries, which its precalc leaves commented out: periodic
+    # keeping the absorbing layer, monopole Dirichlet and monopole radiative, from a seeded
+    # potential on 24^3 with a dissipative layer, 30 substeps
+    n, nx = 2048, 24
+    pos, vel = rg.generate_exp_disk(3, n, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1, 0.0, 0.0)
+    dx = 16.0 / nx
+    c = 10.0 * float(np.max(np.linalg.norm(vel, axis=1)))
+    wave = [1.0 / (4 * dx), 0.3, c, 0, 0, 1e-6, 10 ** 6, 10 ** 6, 3]
+    phi_init = -1.0 + 0.1 * np.random.default_rng(3).standard_normal(nx ** 3)
+    for bc, tag in ((0, "periodic_layer"), (1, "monopole"), (2, "radiative")):
+        wave_bc_case(L, f"ref_wave_bc_{tag}", pos, vel, np.full(n, 1.0 / n), np.full(n, 1e-4),
+                     nx, dx, 0.2, wave, bc, 1.0, (0.1, -0.05, 0.02), phi_init, 30, out)
     for f in sorted(out.glob("ref_*.npz")):
         print(f.name, f.stat().st_size)
 

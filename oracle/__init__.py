@@ -128,6 +128,8 @@ def ref_lib():
                          C.c_double, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp]
     L.ref_wave_bc.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_int, C.c_double, C.c_double, dp,
                               C.c_int, C.c_double, dp, dp, C.c_int, dp, dp]
+    L.ref_nbody_grid.argtypes = [C.c_int64, dp, dp, dp, dp, C.c_double, C.c_int, C.c_int,
+                                 C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp]
     return L
 
 

@@ -195,6 +195,55 @@ int ref_pm(int64_t n, const double* pos, const double* vel, const double* mass,
     }
 }
 
+// NBodyIntegrationSolver with a grid (rrgsim_integration_nbody.cuh:32-48): precalc, nsteps
+// calc_step, then sync_particles_and_grid: CIC mass, the particle potential (recomputed), and
+// the NGP cell averages of the particle potential and acceleration. Outputs: the grid's mass,
+// potential (nx^3) and acceleration (nx^3 x 3); the particles' pos, vel, acc (n x 3) and
+// potential (n).
+int ref_nbody_grid(int64_t n, const double* pos, const double* vel, const double* mass,
+                   const double* soft2, double dt, int nsteps, int nx, double dx,
+                   double bc_frac, double* grid_mass, double* grid_grav, double* grid_acc,
+                   double* pos_out, double* vel_out, double* acc_out, double* grav_out) {
+    try {
+        auto pd = make_particles(n, pos, vel, mass, soft2);
+        auto pctx = rrgsim::common::initialize_particles_context_(pd);
+        auto grid = make_grid(nx, dx, bc_frac);
+        auto gctx = rrgsim::common::initialize_grid_context_(grid);
+        rrgsim::integration::IntegrationParams params;
+        params.sim_params.dt_dynamics = dt;
+        params.sim_params.use_wave_model = false;
+        params.mb_grid_info = grid;
+        std::shared_ptr<rrgsim::integration::IntegrationSolver> solver =
+            std::make_shared<rrgsim::integration::NBodyIntegrationSolver>();
+        solver->init(params, pctx, gctx);
+        solver->precalc();
+        for (int s = 0; s < nsteps; ++s) solver->calc_step();
+        solver->sync_particles_and_grid();
+        const size_t nc = static_cast<size_t>(nx) * nx * nx;
+        if (grid_mass) {
+            auto m = gctx->mass_.to_vector();
+            std::memcpy(grid_mass, m.data(), sizeof(double) * nc);
+        }
+        if (grid_grav) {
+            auto g = gctx->grav_curr_.to_vector();
+            std::memcpy(grid_grav, g.data(), sizeof(double) * nc);
+        }
+        copy3(gctx->acc_.to_vector(), grid_acc);
+        copy3(pctx->pos_.to_vector(), pos_out);
+        copy3(pctx->vel_.to_vector(), vel_out);
+        copy3(pctx->acc_.to_vector(), acc_out);
+        if (grav_out) {
+            auto g = pctx->grav_.to_vector();
+            std::memcpy(grav_out, g.data(), sizeof(double) * n);
+        }
+        RR::CUDA::check(cudaGetLastError(), "ref_nbody_grid");
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 // The reference's wave solver under a non-periodic or layered boundary (wave.cu:18-104, set up
 // by set_boundary_monopole / set_boundary_periodic, :196-228), which its precalc leaves
 // commented out (rrgsim_integration_rect.cuh:57-64): CIC of the particles, the boundary

@@ -82,6 +82,20 @@ def wave_bc_case(L, name, pos, vel, mass, soft2, nx, dx, bc_frac, wave, bc, tota
                         phi_init=phi_init, iterations=iterations, mass0=mass0, phi=phi)
 
 
+def nbody_grid_case(L, name, pos, vel, mass, soft2, dt, steps, nx, dx, bc_frac, out: Path):
+    n = len(mass)
+    nc = nx ** 3
+    gm, gg, ga = np.empty(nc), np.empty(nc), np.empty((nc, 3))
+    p1, v1, a1, g1 = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3)), np.empty(n)
+    rc = L.ref_nbody_grid(n, _p(pos), _p(vel), _p(mass), _p(soft2), dt, steps, nx, dx, bc_frac,
+                          _p(gm), _p(gg), _p(ga), _p(p1), _p(v1), _p(a1), _p(g1))
+    if rc:
+        raise RuntimeError(L.ref_last_error().decode())
+    np.savez_compressed(out / f"{name}.npz", pos=pos, vel=vel, mass=mass, soft2=soft2, dt=dt,
+                        steps=steps, nx=nx, dx=dx, bc_frac=bc_frac, grid_mass=gm, grid_grav=gg,
+                        grid_acc=ga, pos_n=p1, vel_n=v1, acc_n=a1, grav_n=g1)
+
+
 def main():
     out = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent
     out.mkdir(parents=True, exist_ok=True)
@@ -150,6 +164,12 @@ def main():
     for bc, tag in ((0, "periodic_layer"), (1, "monopole"), (2, "radiative")):
         wave_bc_case(L, f"ref_wave_bc_{tag}", pos, vel, np.full(n, 1.0 / n), np.full(n, 1e-4),
                      nx, dx, 0.2, wave, bc, 1.0, (0.1, -0.05, 0.02), phi_init, 30, out)
+    # 8. the N-body strategy with a grid: the sync's CIC mass and NGP cell averages of the
+    # particle potential and acceleration (a disk on 16^3 spanning +-8), after 3 steps
+    n, nx = 4096, 16
+    pos, vel = rg.generate_exp_disk(4, n, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1, 0.0, 0.0)
+    nbody_grid_case(L, "ref_nbody_grid_disk4096_nx16", pos, vel, np.full(n, 1.0 / n),
+                    np.full(n, 1e-4), 1e-3, 3, nx, 16.0 / nx, 0.2, out)
     for f in sorted(out.glob("ref_*.npz")):
         print(f.name, f.stat().st_size)
 

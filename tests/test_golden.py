@@ -99,6 +99,26 @@ def test_oracle_wave_boundaries_match_reference(name):
     assert np.max(np.abs(st.curr - g["phi"])) <= 1e-11 * np.max(np.abs(g["phi"]))
 
 
+NBODY_GRID = "ref_nbody_grid_disk4096_nx16"
+
+
+def test_oracle_nbody_grid_projections_match_reference():
+    g = load(NBODY_GRID)
+    nx, dx = int(g["nx"]), float(g["dx"])
+    og = orc.make_grid(nx, dx, bc_frac=float(g["bc_frac"]))
+    acc0 = orc.direct_acc(g["pos"], g["mass"], g["soft2"])
+    p, v, a = orc.nbody_steps(g["pos"], g["vel"], acc0, g["mass"], g["soft2"], float(g["dt"]),
+                              int(g["steps"]))
+    assert np.max(rel_err(p, g["pos_n"])) <= 1e-12
+    grav = orc.direct_grav(g["pos_n"], g["mass"], g["soft2"])
+    assert np.max(np.abs(grav - g["grav_n"]) / np.abs(g["grav_n"])) <= 1e-12
+    np.testing.assert_allclose(orc.cic_fp64(g["pos_n"], g["mass"], og), g["grid_mass"],
+                               rtol=1e-12, atol=1e-18)
+    for mine, ref in ((orc.ngp_project(g["pos_n"], og, g["grav_n"]), g["grid_grav"]),
+                      (orc.ngp_project(g["pos_n"], og, g["acc_n"]), g["grid_acc"])):
+        assert np.max(np.abs(mine - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
 def test_golden_fixtures_are_nontrivial():
     for name in NBODY + PM:
         g = load(name)
@@ -200,3 +220,38 @@ def test_gpu_wave_boundaries_match_reference(name, prec):
     # (about 1e-9 of its scale after 30 substeps); FP32 adds its own rounding
     tol = 1e-8 if prec == "fp64" else 1e-5
     assert np.max(np.abs(got - g["phi"])) <= tol * np.max(np.abs(g["phi"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_gpu_nbody_grid_projections_match_reference(prec):
+    g = load(NBODY_GRID)
+    nx, dx = int(g["nx"]), float(g["dx"])
+    grid = rg.GridInfo.from_values(nx, dx, float(g["bc_frac"]))
+    sim = rg.SimParams(time_max=1.0, dt_save=1.0, dt_dynamics=float(g["dt"]),
+                       saves_without_dump=2 ** 63, use_wave_model=0)
+    with rg.Context(0, prec) as c:
+        c.load_particles(g["pos"], g["vel"], g["mass"], g["soft2"])
+        c.init_grid(grid)
+        c.solver_init(sim)
+        c.precalc()
+        c.calc_steps(int(g["steps"]))
+        c.sync_particles_and_grid()
+        got = c.get_grid()
+        shift = c.deposit_scale()
+    n = len(g["mass"])
+    if prec == "fp64":
+        # fixed-point deposit: half a step of 2^-S per contribution; NGP sums: atomic order only
+        assert np.max(np.abs(got["mass"] - g["grid_mass"])) <= 0.5 * 8 * n * 2.0 ** -shift
+        for k, ref in (("grav", g["grid_grav"]), ("acc", g["grid_acc"])):
+            assert np.max(np.abs(got[k] - ref)) <= 1e-9 * np.max(np.abs(ref))
+        return
+    # FP32 positions: the CIC weights move by the position's rounding, and a particle within
+    # that rounding of an NGP cell face may land in the neighbouring cell, which changes both
+    # cells' averages; all but a few of the occupied cells agree closely
+    assert np.max(np.abs(got["mass"] - g["grid_mass"])) <= 1e-4 * np.max(g["grid_mass"])
+    occupied = g["grid_grav"] != 0.0
+    for k, ref in (("grav", g["grid_grav"]), ("acc", g["grid_acc"])):
+        err = np.abs(got[k] - ref).reshape(len(occupied), -1).max(axis=1)[occupied]
+        scale = np.abs(ref).reshape(len(occupied), -1).max(axis=1)[occupied]
+        assert np.mean(err <= 1e-4 * scale) >= 0.99

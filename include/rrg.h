@@ -264,7 +264,9 @@ RRG_API rrg_status rrg_calc_conservation(rrg_ctx* ctx, rrg_conservation* out);
 /* calc_mass_center: nbody.cu:293-439, FP64. Synchronises. */
 /* The same reductions, asynchronous: enqueues them on the context stream with a copy of the
  * raw sums (sum m v^2, sum m phi, P[3], L[3], then four zeros) into `sums` (12 doubles of host
- * memory; pinned memory keeps the copy asynchronous) and returns without waiting. Read
+ * memory) and returns without waiting. Pinned memory that the device can address (cudaHostAlloc,
+ * or cudaHostRegister with mapping) receives them from the reduction kernel itself; other host
+ * memory through a copy, asynchronous only when pinned. Read
  * them after the stream has passed that point; rrg_conservation_from_sums converts. No
  * reference counterpart: it lets a host loop overlap the read of one step's diagnostics with
  * the next step. */

@@ -1087,11 +1087,23 @@ RRG_API rrg_status rrg_calc_conservation_async(rrg_ctx* ctx, double* sums) {
         require_particles(ctx);
         RRG_REQUIRE(sums != nullptr, RRG_ERR_INVALID, "NULL output");
         const int rb = conservation_blocks(ctx->n);
+        // pinned host memory that this device can address takes the sums straight from the
+        // finishing kernel: no copy-engine hop between the step's kernels
+        double* out = ctx->red_out.as<double>();
+        bool direct = false;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, sums) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+            at.devicePointer != nullptr) {
+            out = static_cast<double*>(at.devicePointer);
+            direct = true;
+        } else {
+            (void)cudaGetLastError();
+        }
         launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
-                            ctx->red_partial.as<double>(), rb, ctx->red_out.as<double>(),
-                            ctx->stream, false);
-        RRG_CUDA(cudaMemcpyAsync(sums, ctx->red_out.p, 12 * sizeof(double),
-                                 cudaMemcpyDeviceToHost, ctx->stream));
+                            ctx->red_partial.as<double>(), rb, out, ctx->stream, false);
+        if (!direct)
+            RRG_CUDA(cudaMemcpyAsync(sums, ctx->red_out.p, 12 * sizeof(double),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
     })
 }
 

@@ -191,10 +191,17 @@ def test_conservation_sums_do_not_depend_on_particle_order(prec):
     assert ma == mb
 
 
-def test_asynchronous_conservation_sums_equal_the_synchronous_ones():
+@pytest.mark.parametrize("memory", ["pageable", "pinned"])
+def test_asynchronous_conservation_sums_equal_the_synchronous_ones(memory):
+    """Pageable memory gets a copy; pinned memory the device can address gets the sums from
+    the reduction kernel itself."""
     n = 3000
     pos, vel, m, s2 = plummer(n, seed=8)
-    sums = np.full((3, 12), np.nan)
+    if memory == "pinned":
+        torch = pytest.importorskip("torch")
+        sums = torch.full((3, 12), float("nan"), dtype=torch.float64).pin_memory().numpy()
+    else:
+        sums = np.full((3, 12), np.nan)
     with _ctx("fp32", pos, vel, m, s2) as c:
         c.nbody_grav()
         ref = c.calc_conservation()

@@ -2,7 +2,9 @@
 
 The timed value of a multi-GPU run is the maximum over ranks of each rank's elapsed time
 (max_over_ranks), taken between barriers; the reference arm runs on rank 0 alone and the other
-ranks leave at once without forming a process group."""
+ranks leave at once without forming a process group; its one JSON line carries the bench
+contract's keys."""
+import json
 import os
 import socket
 import subprocess
@@ -66,3 +68,30 @@ def test_reference_arm_leaves_at_once_on_other_ranks():
                         "2"], capture_output=True, text=True, env=env, timeout=120, cwd=ROOT)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_prints_the_bench_line():
+    """The reference arm (the CPU restatement on the host cores) prints one JSON line with the
+    bench contract's keys, on the native arm's metric and workload."""
+    import bench
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps",
+                        "1", "--warmup", "3"], capture_output=True, text=True, env=env,
+                       timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["config"]["workload"] == bench.WORKLOAD
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1
+    assert d["warmup"] >= 3 and d["value"] > 0 and d["ms_per_step"] > 0
+    assert d["scaling"] in ("weak", "strong") and d["data"] == "synthetic"
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["kind"] in ("port", "reference")
+    assert cb["unit"] == d["unit"] and cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0

@@ -33,7 +33,9 @@
 //   stencil more than the overlap saved);
 // - each face value as one 64-bit word (value, epoch) that the readers poll directly, with no
 //   fence, counter or second copy: 114 against 95 us per launch (the doubled face bytes and the
-//   re-polls saturate the SM's path to L2).
+//   re-polls saturate the SM's path to L2);
+// - one block of 512 threads (16 rows) per SM on 128^3 instead of two of 256, for a quarter
+//   fewer face bytes per SM: 98.8 against 93.6 us per launch.
 //
 // All blocks must be resident together: the launch is cooperative and the host checks capacity
 // first. Every wait is bounded; one that runs out sets the error word and the block leaves (the

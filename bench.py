@@ -333,11 +333,12 @@ def run_native(args):
     ctx2.calc_steps(2)  # graphs recorded outside the timed region
     ctx2.synchronize()
     # each step's diagnostics come down into pinned host memory asynchronously; the host reads
-    # step k's while steps k + 1 .. k + DEPTH - 1 are queued (DEPTH slots, one CUDA event
-    # each: ~2 ms of GPU work), so a host thread that the shared host deschedules for a moment
-    # does not stall the GPU. The whole leg runs seven times and the median counts: it is timed
-    # on the host clock, and a shared host now and then stretches a run to twice its time.
-    depth = 16
+    # step k's while steps k + 1 .. k + DEPTH - 1 are queued (DEPTH slots, one CUDA event each:
+    # ~10 ms of GPU work, longer than a scheduler time slice on a contended host), so a host
+    # thread that the shared host deschedules for a moment does not stall the GPU. The whole leg
+    # runs seven times and the median counts: it is timed on the host clock, and a shared host
+    # now and then stretches a run to twice its time.
+    depth = 64
     sums = torch.zeros((depth, 12), dtype=torch.float64).pin_memory().numpy()
     done = [torch.cuda.Event() for _ in range(depth)]
     e2e_runs = []

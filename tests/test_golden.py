@@ -193,7 +193,7 @@ def test_gpu_pm_matches_reference(name, prec):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
 @pytest.mark.parametrize("name", WAVE_BC)
 def test_gpu_wave_boundaries_match_reference(name, prec):
     g = load(name)
@@ -217,7 +217,8 @@ def test_gpu_wave_boundaries_match_reference(name, prec):
     assert it == int(g["iterations"])
     # FP64: the int64 fixed-point deposit differs from the reference's FP64 atomics by up to
     # half a step of 2^-S per contribution, which reaches the potential through the source
-    # (about 1e-9 of its scale after 30 substeps); FP32 adds its own rounding
+    # (about 1e-9 of its scale after 30 substeps); FP32 (and MIXED, whose grid is FP32) adds
+    # its own rounding
     tol = 1e-8 if prec == "fp64" else 1e-5
     assert np.max(np.abs(got - g["phi"])) <= tol * np.max(np.abs(g["phi"]))
 

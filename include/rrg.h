@@ -290,6 +290,10 @@ RRG_API rrg_status rrg_solver_init(rrg_ctx* ctx, const rrg_sim_params* sim);
 RRG_API rrg_status rrg_solver_precalc(rrg_ctx* ctx);
 /* calc_step, nsteps times. Fused kernels, replayed as CUDA graphs; advances time and iter. */
 RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps);
+/* Records and instantiates every CUDA graph that the next rrg_solver_calc_steps(ctx, nsteps)
+ * replays, so that call launches without recording. Runs nothing on the device and leaves
+ * the state as it was. No counterpart in the reference (it has no graphs). */
+RRG_API rrg_status rrg_solver_prepare(rrg_ctx* ctx, int nsteps);
 /* sync_particles_and_grid: potential (and, in wave mode, acceleration) on particles. */
 RRG_API rrg_status rrg_solver_sync(rrg_ctx* ctx);
 /* Precalc for a restored state (resume from a dump, wiring read_particles_dump,
@@ -491,8 +495,10 @@ RRG_API rrg_status rrg_dev_direct_vjp_f32(const void* posm, const void* hsoft,
  * plugin inside another framework's allocator, a loop that must not risk an allocation). It
  * allocates nothing: its scratch is one fixed 4 MiB device array per GPU, held until the
  * process exits. n must be in [1, 1048576]; larger n is RRG_ERR_INVALID. The first call on a
- * device looks up that array's device address (make it before any stream capture). All calls
- * share the array: calls that overlap on the GPU race. No counterpart in the reference. */
+ * device looks up that array's device address (make it before any stream capture); the
+ * address is kept for the life of the process, so it does not survive a reset of the device
+ * (cudaDeviceReset, or a primary-context reset by the host framework). All calls share the
+ * array: calls that overlap on the GPU race. No counterpart in the reference. */
 RRG_API rrg_status rrg_dev_direct_forces_f32_noalloc(const void* posm, const void* hsoft,
                                                      float uniform_hsoft, int64_t n, void* out,
                                                      void* stream);

@@ -70,6 +70,8 @@ def lib():
                                     C.c_int]),
             "orc_conservation": (None, [i64, d, d, d, d, d]),
             "orc_mass_center": (None, [i64, d, d, d]),
+            "orc_exp_disk": (None, [C.c_uint64, i64, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, d, d]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -311,3 +313,13 @@ def mass_center(pos, mass):
     out = np.empty(4)
     lib().orc_mass_center(len(mass), _d(pos), _d(mass), _d(out))
     return out[:3].copy(), float(out[3])
+
+
+def exp_disk(seed: int, n: int, disk_mass: float = 1.0, scale_length: float = 1.0,
+             z0: float = 0.1, r_max: float = 7.5, z_max: float = 7.5, disp_frac: float = 0.1):
+    """The benchmark's synthetic exponential disk: the same bits as
+    rrgsim_b200.generate_exp_disk with the same arguments and no bulge."""
+    pos, vel = np.empty((n, 3)), np.empty((n, 3))
+    lib().orc_exp_disk(int(seed), int(n), float(disk_mass), float(scale_length), float(z0),
+                       float(r_max), float(z_max), float(disp_frac), _d(pos), _d(vel))
+    return pos, vel

@@ -460,3 +460,80 @@ void orc_mass_center(int64_t n, const double* pos, const double* mass, double* o
     for (int k = 0; k < 3; ++k) out[k] = M > 0.0 ? s[k] / M : 0.0;
     out[3] = M;
 }
+
+/* ---------------------------------------------------------------------------------------- */
+/* synthetic exponential disk (the generator of rrg_generate_exp_disk, restated) */
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+typedef struct { uint64_t s[4]; } orc_rng;
+
+static void rng_seed(orc_rng* g, uint64_t seed) {
+    uint64_t z = seed;
+    for (int k = 0; k < 4; ++k) {
+        z += 0x9e3779b97f4a7c15ULL;
+        uint64_t x = z;
+        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+        g->s[k] = x ^ (x >> 31);
+    }
+}
+
+static uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+static uint64_t rng_next(orc_rng* g) {
+    uint64_t* s = g->s;
+    const uint64_t r = rotl64(s[1] * 5, 7) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl64(s[3], 45);
+    return r;
+}
+
+static double rng_uniform(orc_rng* g) { return (double)(rng_next(g) >> 11) * 0x1.0p-53; }
+static double rng_uniform_open(orc_rng* g) {
+    return ((double)(rng_next(g) >> 11) + 0.5) * 0x1.0p-53;
+}
+static double rng_normal(orc_rng* g) {
+    const double u1 = rng_uniform_open(g), u2 = rng_uniform(g);
+    return sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
+}
+
+void orc_exp_disk(uint64_t seed, int64_t n, double disk_mass, double scale_length, double z0,
+                  double r_max, double z_max, double disp_frac, double* pos, double* vel) {
+    orc_rng g;
+    rng_seed(&g, seed);
+    const double Rd = scale_length;
+    const double fmx = 1.0 - (1.0 + r_max / Rd) * exp(-r_max / Rd);
+    for (int64_t i = 0; i < n; ++i) {
+        const double u = rng_uniform(&g) * fmx;
+        double lo = 0.0, hi = r_max / Rd;
+        for (int it = 0; it < 80; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if (1.0 - (1.0 + mid) * exp(-mid) < u) lo = mid;
+            else hi = mid;
+        }
+        const double R = 0.5 * (lo + hi) * Rd;
+        const double ph = 2.0 * M_PI * rng_uniform(&g);
+        double z;
+        do {
+            const double w = rng_uniform_open(&g);
+            z = z0 * atanh(2.0 * w - 1.0);
+        } while (!(fabs(z) < z_max));
+        const double c = cos(ph), s = sin(ph);
+        pos[3 * i] = R * c;
+        pos[3 * i + 1] = R * s;
+        pos[3 * i + 2] = z;
+        const double x = R / Rd;
+        const double menc = disk_mass * (1.0 - (1.0 + x) * exp(-x));
+        const double vc = R > 0 ? sqrt(1.0 * menc / R) : 0.0;
+        const double sig = disp_frac * vc;
+        vel[3 * i] = -vc * s + sig * rng_normal(&g);
+        vel[3 * i + 1] = vc * c + sig * rng_normal(&g);
+        vel[3 * i + 2] = sig * rng_normal(&g);
+    }
+}

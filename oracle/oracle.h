@@ -104,6 +104,15 @@ void orc_conservation(int64_t n, const double* pos, const double* vel, const dou
 /* calc_mass_center: nbody.cu:293-439. out = {cx, cy, cz, M} */
 void orc_mass_center(int64_t n, const double* pos, const double* mass, double* out);
 
+/* The benchmark's synthetic exponential disk (no bulge), restated here so that the timed CPU
+ * arm needs nothing of the product library: xoshiro256** seeded through SplitMix64; R from the
+ * truncated enclosed-mass CDF 1 - (1 + x) e^-x by 80 bisection steps; z = z0 atanh(2w - 1)
+ * below z_max; circular speed sqrt(M(<R) / R) plus Gaussian dispersion (Box-Muller). Draw for
+ * draw and operation for operation the generator of rrg_generate_exp_disk, so the same seed
+ * gives the same bits. pos, vel: n x 3. */
+void orc_exp_disk(uint64_t seed, int64_t n, double disk_mass, double scale_length, double z0,
+                  double r_max, double z_max, double disp_frac, double* pos, double* vel);
+
 #ifdef __cplusplus
 }
 #endif

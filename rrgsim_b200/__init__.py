@@ -145,6 +145,7 @@ def lib() -> C.CDLL:
         "rrg_solver_init": (st, [vp, C.POINTER(SimParams)]),
         "rrg_solver_precalc": (st, [vp]),
         "rrg_solver_calc_steps": (st, [vp, i32]),
+        "rrg_solver_prepare": (st, [vp, i32]),
         "rrg_solver_sync": (st, [vp]),
         "rrg_solver_resume": (st, [vp]),
         "rrg_get_wave_state": (st, [vp, d, d]),
@@ -251,12 +252,22 @@ class Context:
         self._c(lib().rrg_load_particles(self._h, n, _d(pos), _d(vel), _d(mass), _d(soft2)))
         self.n = n
 
-    def get_particles(self) -> dict:
+    def get_particles(self, out: dict | None = None) -> dict:
+        """The particle state in the original order. With `out`, only the arrays it holds
+        ("pos", "vel", "acc": float64 (n, 3) C-contiguous; "grav": float64 (n,)) are
+        written, in place (pinned host arrays make the copies direct)."""
         n = self.n
-        pos, vel, acc = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
-        grav = np.empty(n)
-        self._c(lib().rrg_get_particles(self._h, _d(pos), _d(vel), _d(acc), _d(grav)))
-        return {"pos": pos, "vel": vel, "acc": acc, "grav": grav}
+        if out is None:
+            out = {"pos": np.empty((n, 3)), "vel": np.empty((n, 3)), "acc": np.empty((n, 3)),
+                   "grav": np.empty(n)}
+        for k, a in out.items():
+            want = (n,) if k == "grav" else (n, 3)
+            if (k not in ("pos", "vel", "acc", "grav") or a.dtype != np.float64 or
+                    a.shape != want or not a.flags.c_contiguous):
+                raise RRGError(1, f"get_particles: out[{k!r}] must be float64 {want}, contiguous")
+        self._c(lib().rrg_get_particles(self._h, *(_d(out[k]) if k in out else None
+                                                   for k in ("pos", "vel", "acc", "grav"))))
+        return out
 
     def time(self):
         t = C.c_double()
@@ -370,6 +381,10 @@ class Context:
 
     def calc_steps(self, nsteps: int) -> None:
         self._c(lib().rrg_solver_calc_steps(self._h, int(nsteps)))
+
+    def prepare_steps(self, nsteps: int) -> None:
+        """Records the CUDA graphs the next calc_steps(nsteps) replays; runs nothing."""
+        self._c(lib().rrg_solver_prepare(self._h, int(nsteps)))
 
     def sync_particles_and_grid(self) -> None:
         self._c(lib().rrg_solver_sync(self._h))

@@ -78,6 +78,8 @@ struct Buf {
 struct GraphExec {
     cudaGraphExec_t exec = nullptr;
     uint64_t kernels = 0;
+    // the context's grid flags after the recorded steps, set again at every replay
+    bool src_dirty = false, src_valid = true, wave_solve_used = false;
 };
 
 }  // namespace rrg
@@ -125,7 +127,7 @@ struct rrg_ctx {
     bool wave_solve_used = false;
 
     // reductions / transfers
-    Buf red_partial, red_out, dl;
+    Buf red_partial, red_out, dl, chk;
     double* host_red = nullptr;
 
     // solver
@@ -521,7 +523,9 @@ void wave_steps_unfused(rrg_ctx* c, int nsteps) {
     }
 }
 
-void run_graph(rrg_ctx* c, int nsteps) {
+// The executable graph of the next `nsteps`-step chunk, recorded and instantiated on first use
+// (recording launches nothing); advances the buffer roles and flags as running the chunk does.
+GraphExec& chunk_graph(rrg_ctx* c, int nsteps) {
     bool prologue = true;
     if (c->wave_mode && c->pending) {
         // adopt the prediction the previous chunk left
@@ -564,6 +568,9 @@ void run_graph(rrg_ctx* c, int nsteps) {
         cudaError_t e = cudaGraphInstantiate(&ge.exec, g, 0);
         cudaGraphDestroy(g);
         RRG_CUDA(e);
+        ge.src_dirty = c->src_dirty;
+        ge.src_valid = c->src_valid;
+        ge.wave_solve_used = c->wave_solve_used;
         it = c->graphs.emplace(key, ge).first;
     } else {
         // replaying: advance the buffer roles exactly as recording did
@@ -571,13 +578,54 @@ void run_graph(rrg_ctx* c, int nsteps) {
             const int flips = prologue ? nsteps : nsteps - 1;
             c->mg_cur = (flips % 2 == 1) ? 1 - mg0 : mg0;
             if (c->wave.iterations % 2 == 1) c->phi_cur = (nsteps % 2 == 1) ? 1 - phi0 : phi0;
+            c->src_dirty = it->second.src_dirty;
+            c->src_valid = it->second.src_valid;
+            c->wave_solve_used = c->wave_solve_used || it->second.wave_solve_used;
         } else {
             c->cur = ((nsteps - 1) % 2 == 1) ? 1 - cur0 : cur0;
         }
     }
-    RRG_CUDA(cudaGraphLaunch(it->second.exec, c->stream));
-    count_launches(it->second.kernels);
     if (c->wave_mode) c->pending = true;
+    return it->second;
+}
+
+void run_graph(rrg_ctx* c, int nsteps) {
+    GraphExec& ge = chunk_graph(c, nsteps);
+    RRG_CUDA(cudaGraphLaunch(ge.exec, c->stream));
+    count_launches(ge.kernels);
+}
+
+// The chunks a calc_steps(nsteps) call runs, in order: at most 64 steps each, and in wave mode
+// cut at every re-sort of the particles by cell (every `interval` steps). `each(chunk, sort)`
+// is called per chunk; `sort` is true when the particles are re-sorted before it.
+template <typename F>
+void for_each_chunk(rrg_ctx* c, int nsteps, int64_t& steps_since_sort, F each) {
+    // long runs are recorded once per chunk length and replayed; in wave mode the particles are
+    // re-sorted by cell between chunks every sort_interval steps (64: the deposit sorts a
+    // disordered warp by cell itself, so only the gathers' locality degrades between sorts;
+    // 16, 32 and 64 steps measured 125.7, 124.0 and 123.2 us per step on the 2^20-particle
+    // disk)
+    const int interval = c->wave_mode ? (c->sort_interval < 0 ? 64 : c->sort_interval) : 0;
+    int left = nsteps;
+    while (left > 0) {
+        int chunk = std::min(left, 64);
+        bool sort = false;
+        if (interval > 0) {
+            if (steps_since_sort >= interval) {
+                sort = true;
+                steps_since_sort = 0;
+            }
+            chunk = static_cast<int>(std::min<int64_t>(chunk, interval - steps_since_sort));
+        }
+        each(chunk, sort);
+        steps_since_sort += chunk;
+        left -= chunk;
+    }
+}
+
+bool checks_inside_steps(const rrg_ctx* c) {
+    return c->wave_mode && c->wave.steady_check_step > 0 &&
+           c->wave.iterations > c->wave.steady_check_step;
 }
 
 }  // namespace
@@ -661,24 +709,52 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
                     "rrg_load_particles: n must be < 2^31");
         RRG_REQUIRE(pos && vel && mass && soft2, RRG_ERR_INVALID,
                     "rrg_load_particles: NULL array");
-        double mmax = 0.0;
-        for (int64_t i = 0; i < n; ++i) {
-            for (int k = 0; k < 3; ++k) {
-                RRG_REQUIRE(std::isfinite(pos[3 * i + k]) && std::isfinite(vel[3 * i + k]),
-                            RRG_ERR_INVALID,
-                            "rrg_load_particles: non-finite position/velocity at particle " +
-                                std::to_string(i));
-            }
-            RRG_REQUIRE(std::isfinite(mass[i]) && mass[i] >= 0.0, RRG_ERR_INVALID,
-                        "rrg_load_particles: bad mass at particle " + std::to_string(i));
-            RRG_REQUIRE(std::isfinite(soft2[i]) && soft2[i] >= 0.0, RRG_ERR_INVALID,
-                        "rrg_load_particles: bad soft2 at particle " + std::to_string(i));
-            mmax = std::max(mmax, mass[i]);
+
+        // stage the FP64 host arrays on the device and check them there: the lowest index of
+        // a non-finite position or velocity, of a mass or softening that is negative or not
+        // finite; the largest mass; whether masses and softenings are uniform. Nothing of the
+        // context changes before the checks pass.
+        const size_t stage = static_cast<size_t>(n) * 8 * sizeof(double);
+        ensure_download(ctx, stage);
+        double* d = ctx->dl.as<double>();
+        RRG_CUDA(cudaMemcpyAsync(d, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        RRG_CUDA(cudaMemcpyAsync(d + 3 * n, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        RRG_CUDA(cudaMemcpyAsync(d + 6 * n, mass, n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        RRG_CUDA(cudaMemcpyAsync(d + 7 * n, soft2, n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        if (!ctx->chk.p) ctx->chk.alloc(sizeof(LoadCheck));
+        RRG_CUDA(cudaMemsetAsync(ctx->chk.p, 0, sizeof(LoadCheck), ctx->stream));
+        launch_check_state(n, d, d + 3 * n, d + 6 * n, d + 7 * n, ctx->chk.as<LoadCheck>(),
+                           ctx->sms, ctx->stream);
+        LoadCheck ck;
+        RRG_CUDA(cudaMemcpyAsync(ctx->host_red, ctx->chk.p, sizeof(LoadCheck),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::memcpy(&ck, ctx->host_red, sizeof(LoadCheck));
+        {
+            // the lowest offending particle; at one particle positions and velocities are
+            // reported first, then the mass, then the softening
+            const int64_t none = INT64_MAX;
+            const auto at = [&](unsigned int v) {
+                return v ? static_cast<int64_t>(0xffffffffu - v) : none;
+            };
+            const int64_t ipv = at(ck.bad_pv), im = at(ck.bad_mass), is = at(ck.bad_soft);
+            const int64_t first = std::min(ipv, std::min(im, is));
+            RRG_REQUIRE(first == none || first != ipv, RRG_ERR_INVALID,
+                        "rrg_load_particles: non-finite position/velocity at particle " +
+                            std::to_string(first));
+            RRG_REQUIRE(first == none || first != im, RRG_ERR_INVALID,
+                        "rrg_load_particles: bad mass at particle " + std::to_string(first));
+            RRG_REQUIRE(first == none, RRG_ERR_INVALID,
+                        "rrg_load_particles: bad soft2 at particle " + std::to_string(first));
         }
-        bool uniform = true;
-        for (int64_t i = 1; i < n && uniform; ++i) uniform = (soft2[i] == soft2[0]);
-        bool umass = true;
-        for (int64_t i = 1; i < n && umass; ++i) umass = (mass[i] == mass[0]);
+        double mmax = 0.0;
+        std::memcpy(&mmax, &ck.mass_max_bits, sizeof(double));
+        const bool uniform = ck.soft_varies == 0;
+        const bool umass = ck.mass_varies == 0;
         ctx->uniform_mass = umass ? mass[0] : -1.0;
 
         // recorded graphs stay valid when the new particles reuse every buffer and launch value
@@ -734,18 +810,7 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
             ctx->uniform_hsoft != hsoft_before || ctx->soft_uniform != uniform_before)
             drop_graphs(ctx);
 
-        // stage the FP64 host arrays, then pack on the device
-        const size_t stage = static_cast<size_t>(n) * 8 * sizeof(double);
-        ensure_download(ctx, stage);
-        double* d = ctx->dl.as<double>();
-        RRG_CUDA(cudaMemcpyAsync(d, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-        RRG_CUDA(cudaMemcpyAsync(d + 3 * n, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-        RRG_CUDA(cudaMemcpyAsync(d + 6 * n, mass, n * sizeof(double), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-        RRG_CUDA(cudaMemcpyAsync(d + 7 * n, soft2, n * sizeof(double), cudaMemcpyHostToDevice,
-                                 ctx->stream));
+        // pack the staged arrays into the device state
         launch_pack_state(ctx->prec, n, d, d + 3 * n, d + 6 * n, d + 7 * n, ctx->posm[0].p,
                           ctx->poslo[0].p, ctx->vel.p, uniform ? nullptr : ctx->hsoft.p,
                           ctx->stream);
@@ -1244,10 +1309,7 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
         RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
         RRG_REQUIRE(nsteps >= 0, RRG_ERR_INVALID, "nsteps must be >= 0");
         if (nsteps > 0) {
-            const bool checks_inside =
-                ctx->wave_mode && ctx->wave.steady_check_step > 0 &&
-                ctx->wave.iterations > ctx->wave.steady_check_step;
-            if (checks_inside) {
+            if (checks_inside_steps(ctx)) {
                 drop_pending(ctx);
                 wave_steps_unfused(ctx, nsteps);
             } else {
@@ -1256,31 +1318,42 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
                     RRG_CUDA(cudaMemsetAsync(ctx->mg[1 - ctx->mg_cur].p, 0,
                                              ctx->mg[1 - ctx->mg_cur].bytes, ctx->stream));
                 }
-                // long runs are recorded once per chunk length and replayed; in wave mode the
-                // particles are re-sorted by cell between chunks every sort_interval steps
-                // (64: the deposit sorts a disordered warp by cell itself, so only the
-                // gathers' locality degrades between sorts; 16, 32 and 64 steps measured 125.7,
-                // 124.0 and 123.2 us per step on the 2^20-particle disk)
-                const int interval =
-                    ctx->wave_mode ? (ctx->sort_interval < 0 ? 64 : ctx->sort_interval) : 0;
-                int left = nsteps;
-                while (left > 0) {
-                    int chunk = std::min(left, 64);
-                    if (interval > 0) {
-                        if (ctx->steps_since_sort >= interval)
-                            sort_particles(ctx);  // (a pending prediction is permuted along)
-                        chunk = static_cast<int>(
-                            std::min<int64_t>(chunk, interval - ctx->steps_since_sort));
-                    }
+                for_each_chunk(ctx, nsteps, ctx->steps_since_sort, [&](int chunk, bool sort) {
+                    if (sort) sort_particles(ctx);  // (a pending prediction is permuted along)
                     run_graph(ctx, chunk);
-                    ctx->steps_since_sort += chunk;
-                    left -= chunk;
-                }
+                });
             }
             for (int s = 0; s < nsteps; ++s) {
                 ctx->iter += 1;
                 ctx->time += ctx->sim.dt_dynamics;
             }
+        }
+    })
+}
+
+RRG_API rrg_status rrg_solver_prepare(rrg_ctx* ctx, int nsteps) {
+    RRG_ENTRY(ctx, {
+        RRG_REQUIRE(ctx->solver_ready, RRG_ERR_STATE, "rrg_solver_init first");
+        RRG_REQUIRE(nsteps >= 0, RRG_ERR_INVALID, "nsteps must be >= 0");
+        if (nsteps > 0 && !checks_inside_steps(ctx)) {
+            // walk the chunks of that call, recording what is missing, then put the roles back
+            const int cur = ctx->cur, mg_cur = ctx->mg_cur, phi_cur = ctx->phi_cur;
+            const bool pending = ctx->pending, src_dirty = ctx->src_dirty,
+                       src_valid = ctx->src_valid, used = ctx->wave_solve_used;
+            int64_t since = ctx->steps_since_sort;
+            try {
+                for_each_chunk(ctx, nsteps, since, [&](int chunk, bool) {
+                    chunk_graph(ctx, chunk);
+                });
+            } catch (...) {
+                ctx->cur = cur, ctx->mg_cur = mg_cur, ctx->phi_cur = phi_cur;
+                ctx->pending = pending, ctx->src_dirty = src_dirty, ctx->src_valid = src_valid;
+                ctx->wave_solve_used = used;
+                throw;
+            }
+            ctx->cur = cur, ctx->mg_cur = mg_cur, ctx->phi_cur = phi_cur;
+            ctx->pending = pending, ctx->src_dirty = src_dirty, ctx->src_valid = src_valid;
+            ctx->wave_solve_used = used;
         }
     })
 }
@@ -1349,10 +1422,13 @@ RRG_API rrg_status rrg_dev_direct_forces_f32(const void* posm, const void* poslo
         L.epi.acc = out;
         L.splits = direct_choose_splits(precision, n, num_sms(dev));
         L.scratch_bytes = direct_scratch_bytes(precision, n, L.splits);
+        // the split partials are float4 records: they start on a 256-byte boundary behind the
+        // potential whatever n is
+        const size_t pot_bytes = (sizeof(float) * static_cast<size_t>(n) + 255) & ~size_t(255);
         void* pot = nullptr;
-        RRG_CUDA(cudaMallocAsync(&pot, sizeof(float) * n + L.scratch_bytes, s));
+        RRG_CUDA(cudaMallocAsync(&pot, pot_bytes + L.scratch_bytes, s));
         L.epi.pot = pot;
-        L.scratch = L.scratch_bytes ? static_cast<char*>(pot) + sizeof(float) * n : nullptr;
+        L.scratch = L.scratch_bytes ? static_cast<char*>(pot) + pot_bytes : nullptr;
         L.stream = s;
         try {
             launch_direct(L);

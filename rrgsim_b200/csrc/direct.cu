@@ -580,6 +580,8 @@ void launch_direct(const DirectLaunch& L) {
     const int real_splits = static_cast<int>((tiles + tiles_per - 1) / tiles_per);
     RRG_REQUIRE(real_splits <= 1 || L.scratch_bytes >= direct_scratch_bytes(L.prec, L.n, real_splits),
                 RRG_ERR_INVALID, "direct sum: scratch too small for the split count");
+    RRG_REQUIRE(real_splits <= 1 || (reinterpret_cast<uintptr_t>(L.scratch) & 15u) == 0,
+                RRG_ERR_INVALID, "direct sum: split partials must start on a 16-byte boundary");
     const bool usoft = (L.hsoft == nullptr);
     const int variant = (L.prec == RRG_PREC_FP32 && L.variant >= 1 && L.variant <= 4)
                             ? L.variant

@@ -191,6 +191,49 @@ __global__ void __launch_bounds__(kRedThreads) conservation_finish(
     }
 }
 
+// Validity of uploaded particles, the largest mass and whether masses and softenings are
+// uniform: grid-stride over the flat arrays (coalesced), one warp reduction and one atomic per
+// warp and quantity.
+__global__ void __launch_bounds__(256) check_state_kernel(
+    int64_t n, const double* __restrict__ pos3, const double* __restrict__ vel3,
+    const double* __restrict__ mass, const double* __restrict__ soft2, LoadCheck* chk) {
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    unsigned int bad_pv = 0, bad_m = 0, bad_s = 0, mv = 0, sv = 0;
+    double mmax = 0.0;
+    for (int64_t k = t0; k < 3 * n; k += stride) {
+        if (!isfinite(__ldg(pos3 + k)) || !isfinite(__ldg(vel3 + k)))
+            bad_pv = max(bad_pv, 0xffffffffu - static_cast<unsigned int>(k / 3));
+    }
+    const double m0 = __ldg(mass), s0 = __ldg(soft2);
+    for (int64_t i = t0; i < n; i += stride) {
+        const double m = __ldg(mass + i), h = __ldg(soft2 + i);
+        if (!(isfinite(m) && m >= 0.0)) bad_m = max(bad_m, 0xffffffffu - static_cast<unsigned int>(i));
+        else mmax = fmax(mmax, m);
+        if (!(isfinite(h) && h >= 0.0)) bad_s = max(bad_s, 0xffffffffu - static_cast<unsigned int>(i));
+        mv |= (m != m0);
+        sv |= (h != s0);
+    }
+    bad_pv = __reduce_max_sync(0xffffffffu, bad_pv);
+    bad_m = __reduce_max_sync(0xffffffffu, bad_m);
+    bad_s = __reduce_max_sync(0xffffffffu, bad_s);
+    mv = __reduce_or_sync(0xffffffffu, mv);
+    sv = __reduce_or_sync(0xffffffffu, sv);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mmax = fmax(mmax, __shfl_xor_sync(0xffffffffu, mmax, o));
+    if ((threadIdx.x & 31) == 0) {
+        if (bad_pv) atomicMax(&chk->bad_pv, bad_pv);
+        if (bad_m) atomicMax(&chk->bad_mass, bad_m);
+        if (bad_s) atomicMax(&chk->bad_soft, bad_s);
+        if (mv) atomicOr(&chk->mass_varies, 1u);
+        if (sv) atomicOr(&chk->soft_varies, 1u);
+        // non-negative doubles order as their bit patterns
+        if (mmax > 0.0)
+            atomicMax(&chk->mass_max_bits,
+                      static_cast<unsigned long long>(__double_as_longlong(mmax)));
+    }
+}
+
 // Host FP64 AoS -> device state.
 template <typename R, bool MIXED>
 __global__ void pack_kernel(int64_t n, const double* __restrict__ pos3,
@@ -324,6 +367,13 @@ void launch_conservation(int prec, int64_t n, const void* posm, const void* posl
 #undef RRG_CONS
     RRG_LAUNCHED();
     conservation_finish<<<kRedVals, kRedThreads, 0, s>>>(partial, nblocks, out);
+    RRG_LAUNCHED();
+}
+
+void launch_check_state(int64_t n, const double* pos3, const double* vel3, const double* mass,
+                        const double* soft2, LoadCheck* chk, int sms, cudaStream_t s) {
+    const int b = std::max(1, std::min(div_up(3 * n, 256), 4 * sms));
+    check_state_kernel<<<b, 256, 0, s>>>(n, pos3, vel3, mass, soft2, chk);
     RRG_LAUNCHED();
 }
 

@@ -72,6 +72,19 @@ void launch_conservation(int prec, int64_t n, const void* posm, const void* posl
                          double* out, cudaStream_t s, bool com);
 int conservation_blocks(int64_t n);
 
+// Checks of an upload of particles (rrg_load_particles) on the device. Offending indices are
+// stored as 0xffffffff - i under an atomic maximum, so 0 means none and the lowest i wins.
+struct LoadCheck {
+    unsigned int bad_pv, bad_mass, bad_soft;  // non-finite position / velocity; mass or soft2
+                                              // negative or not finite
+    unsigned int mass_varies, soft_varies;    // some mass (soft2) differs from the first
+    unsigned int pad;
+    unsigned long long mass_max_bits;         // bit pattern of the largest valid mass (>= 0)
+};
+// chk must be zeroed before the launch.
+void launch_check_state(int64_t n, const double* pos3, const double* vel3, const double* mass,
+                        const double* soft2, LoadCheck* chk, int sms, cudaStream_t s);
+
 // Conversions between the host FP64 AoS layout and the device state.
 void launch_pack_state(int prec, int64_t n, const double* pos3, const double* vel3,
                        const double* mass, const double* soft2, void* posm, void* poslo,
@@ -111,6 +124,29 @@ void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, co
                       const WaveCoef& c, unsigned long long* maxbits, cudaStream_t s);
 // a = -grad phi on the grid (rm_p2mesh.cu:238-290): acc4[c] = (ax, ay, az, phi[c]).
 void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, cudaStream_t s);
+// One damped-wave update of four x-cells (wave_diss_iteration, wave.cu:106-193, periodic box,
+// uniform coefficients): new = K_MAIN (sum of the six neighbours) + K_ACTUAL phi + K_OLD phi_old
+// + K_F src. Every rounding is written out, so every FP32 kernel that uses it (one launch per
+// substep, the persistent solves, whichever block computes a cell) gives the same bits.
+__device__ __forceinline__ float wave_cell(float a, float b, float ym, float yp, float zm,
+                                           float zp, float c, float po, float s, float km,
+                                           float ka, float ko, float kf) {
+    const float nb = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(a, b), ym), yp), zm), zp);
+    return __fmaf_rn(s, kf, __fmaf_rn(po, ko, __fmaf_rn(c, ka, __fmul_rn(nb, km))));
+}
+// c: four cells of a row; lft / rgt: the cells left of c.x and right of c.w
+__device__ __forceinline__ float4 wave_cell4(const float4 c, float lft, float rgt,
+                                             const float4 ym, const float4 yp, const float4 zm,
+                                             const float4 zp, const float4 po, const float4 s,
+                                             float km, float ka, float ko, float kf) {
+    float4 o;
+    o.x = wave_cell(lft, c.y, ym.x, yp.x, zm.x, zp.x, c.x, po.x, s.x, km, ka, ko, kf);
+    o.y = wave_cell(c.x, c.z, ym.y, yp.y, zm.y, zp.y, c.y, po.y, s.y, km, ka, ko, kf);
+    o.z = wave_cell(c.y, c.w, ym.z, yp.z, zm.z, zp.z, c.z, po.z, s.z, km, ka, ko, kf);
+    o.w = wave_cell(c.z, rgt, ym.w, yp.w, zm.w, zp.w, c.w, po.w, s.w, km, ka, ko, kf);
+    return o;
+}
+
 // One PM step's whole FP32 wave solve in one persistent cooperative kernel (wave_solve.cu):
 // source from the deposit mg (mg_zero cleared), `iterations` substeps over the levels phi0 /
 // phi1 (cur: which holds the current level; the result lands in phi[cur ^ (iterations & 1)],

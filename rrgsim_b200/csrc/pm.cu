@@ -415,11 +415,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) wave_periodic_x4_kernel(
             const float4 zm = pv[k], zp = pv[k + 2];
             const float4 po = old4[o];
             const float4 s = __ldg(src4 + o);
-            float4 out;
-            out.x = (lft + c.y + ym.x + yp.x + zm.x + zp.x) * km + c.x * ka + po.x * ko + s.x * kf;
-            out.y = (c.x + c.z + ym.y + yp.y + zm.y + zp.y) * km + c.y * ka + po.y * ko + s.y * kf;
-            out.z = (c.y + c.w + ym.z + yp.z + zm.z + zp.z) * km + c.z * ka + po.z * ko + s.z * kf;
-            out.w = (c.z + rgt + ym.w + yp.w + zm.w + zp.w) * km + c.w * ka + po.w * ko + s.w * kf;
+            const float4 out = wave_cell4(c, lft, rgt, ym, yp, zm, zp, po, s, km, ka, ko, kf);
             old4[o] = out;
             if constexpr (CHECK) {
                 // differences in FP64, as the scalar kernels take them

@@ -43,6 +43,7 @@
 // turns the word into an error, clears the sync memory. The arithmetic is that of
 // wave_source_kernel<float>, wave_periodic_x4_kernel and gradient_x4_kernel, expression for
 // expression, so the results are the same bits.
+#include <algorithm>
 #include <cstdlib>
 #include <mutex>
 
@@ -258,12 +259,7 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
         const float4 ym = tile[(k * (RB + 2) + r) * W + q];
         const float4 yp = tile[(k * (RB + 2) + r + 2) * W + q];
         const float4 po = old[k], sv = srcs[k * kThreads + tid];
-        float4 out;
-        out.x = (lft + c.y + ym.x + yp.x + zm.x + zp.x) * a.km + c.x * a.ka + po.x * a.ko + sv.x * a.kf;
-        out.y = (c.x + c.z + ym.y + yp.y + zm.y + zp.y) * a.km + c.y * a.ka + po.y * a.ko + sv.y * a.kf;
-        out.z = (c.y + c.w + ym.z + yp.z + zm.z + zp.z) * a.km + c.z * a.ka + po.z * a.ko + sv.z * a.kf;
-        out.w = (c.z + rgt + ym.w + yp.w + zm.w + zp.w) * a.km + c.w * a.ka + po.w * a.ko + sv.w * a.kf;
-        return out;
+        return wave_cell4(c, lft, rgt, ym, yp, zm, zp, po, sv, a.km, a.ka, a.ko, a.kf);
     };
 
     // ---- substeps --------------------------------------------------------------------------
@@ -343,6 +339,377 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     // the counter ends at e0 + iterations in every block: the next launch starts from there
 }
 
+
+// ================================================================================================
+// Two substeps per exchange (nx = 128): temporal blocking with a halo two cells deep.
+//
+// A block of 512 threads (one block per SM, 128 blocks) owns RB = 16 rows x ZC = 8 planes of
+// whole x-rows; a warp is one row. A thread keeps its row's float4 column over the planes
+// z0 - 1 .. z0 + ZC (its own ZC planes and one on either side) in registers, current and
+// previous level. One exchange brings level t of the neighbours two cells deep: rows
+// y0 - 2 .. y0 - 1 and y0 + RB .. y0 + RB + 1 at the own planes, planes z0 - 2 .. z0 - 1 and
+// z0 + ZC .. z0 + ZC + 1 of the own rows, and the four edge rows (y0 - 1 or y0 + RB, z0 - 1 or
+// z0 + ZC) from the diagonal neighbours. Substep A then advances the ten-plane columns and the
+// two rows just outside the block (y0 - 1 and y0 + RB at the own planes: one warp per row and
+// plane, sixteen in all) to level t + 1; substep B advances the block's own cells to t + 2 from
+// those. A cell outside the block is computed from the same values, by the same expression
+// (wave_cell4), as its owner computes it, so the results are the bits of one exchange per
+// substep. Per two substeps: one exchange instead of two, for 19 float4 updates per thread
+// instead of 16, and 48 KB of faces stored per block (an SM of the one-exchange kernel stores
+// 64 KB in two substeps).
+//
+// Shared memory (225,280 bytes): the level tile [KP planes][RB + 4 rows][W], the planes
+// z0 - 2 and z0 + ZC + 1 of the own rows, the columns' source [KP][T], and for the two outer
+// rows their source and, double-buffered, their previous level. An odd substep count ends with
+// one substep B on its own. Every pass ends with an exchange, the last one giving the gradient
+// its halo; a block writes its levels to global memory only after it, so every neighbour has
+// read its initial halo from there by then.
+namespace tb {
+constexpr int T = 512;
+constexpr int W = 32;
+constexpr int NX = 4 * W;
+constexpr int RB = T / W;                 // 16 rows
+constexpr int ZC = kZC;                   // 8 planes
+constexpr int KP = ZC + 2;                // planes of a thread's column: z0 - 1 .. z0 + ZC
+constexpr int JR = RB + 4;                // tile rows: y0 - 2 .. y0 + RB + 1
+constexpr int tileN = KP * JR * W;
+constexpr int zhN = 2 * RB * W;
+constexpr int srcN = KP * T;
+constexpr int ringN = 2 * ZC * W;         // rows y0 - 1 (side 0) and y0 + RB (side 1)
+constexpr size_t smem = static_cast<size_t>(tileN + zhN + srcN + 3 * ringN) * sizeof(float4);
+constexpr int FY = 2 * ZC * W;            // y face: two rows x ZC planes, [row][plane][W]
+constexpr int FZ = 2 * RB * W;            // z face: two planes x RB rows, [plane][row][W]
+constexpr int FB = 2 * FY + 2 * FZ;       // a block's faces per epoch parity: F0 F1 F2 F3
+constexpr int HALO = 2 * FY + 2 * FZ + 4 * W;  // float4 a block copies in per exchange
+static_assert(2 * ZC == T / 32, "one warp per outer row and plane");
+}  // namespace tb
+
+size_t sync_bytes_tb(int64_t nblocks) {
+    return kFaceOffset + static_cast<size_t>(nblocks) * 2 * tb::FB * sizeof(float4);
+}
+
+__global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs a) {
+    using namespace tb;
+    extern __shared__ __align__(16) float4 sm[];
+    float4* const tile = sm;              // [KP][JR][W]: plane z0 - 1 + k, row y0 - 2 + j
+    float4* const zh = tile + tileN;      // [2][RB][W]: planes z0 - 2, z0 + ZC + 1
+    float4* const srcs = zh + zhN;        // [KP][T]
+    float4* const rsrc = srcs + srcN;     // [2 sides][ZC][W]: the outer rows' source
+    float4* const rold = rsrc + ringN;    // [2 parities][2 sides][ZC][W]: their earlier level
+    __shared__ int fail_s;
+    __shared__ unsigned int base_s;
+
+    const int gx = gridDim.x, gz = gridDim.y, bx = blockIdx.x, bz = blockIdx.y;
+    const int me = bz * gx + bx, nblocks = gx * gz;
+    volatile unsigned int* const err = a.sync + kErrWord;
+    unsigned int* const counter = a.sync + me * kCounterStride;
+    if (threadIdx.x == 0) {
+        fail_s = *err != 0;  // an earlier launch failed: invalid until the host resets
+        base_s = *reinterpret_cast<volatile unsigned int*>(counter);
+    }
+    __syncthreads();
+    if (fail_s) return;
+    const unsigned int base = base_s;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r = warp, q = lane;
+    const int y0 = bx * RB, z0 = bz * ZC;
+    const int lsrc = (lane + 31) & 31, rsrcl = (lane + 1) & 31;
+    const int bxm = bx == 0 ? gx - 1 : bx - 1, bxp = bx + 1 == gx ? 0 : bx + 1;
+    const int bzm = bz == 0 ? gz - 1 : bz - 1, bzp = bz + 1 == gz ? 0 : bz + 1;
+    float4* const faces = reinterpret_cast<float4*>(reinterpret_cast<char*>(a.sync) + kFaceOffset);
+    auto face = [&](unsigned int e, int block) {
+        return faces + (static_cast<size_t>(e & 1u) * nblocks + block) * FB;
+    };
+    auto T4 = [&](int k, int j) { return tile + (k * JR + j) * W; };
+    auto g4 = [](int z, int yy) -> size_t {  // float4 index of (0, yy, z), periodic
+        return (static_cast<size_t>(z & (NX - 1)) * NX + (yy & (NX - 1))) * W;
+    };
+    const float km = a.km, ka = a.ka, ko = a.ko, kf = a.kf;
+    const float4* const c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
+    const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
+    const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
+    // the source of four cells from the deposit (wave_source_kernel<float>'s expression)
+    auto source = [&](size_t o4) -> float4 {
+        const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
+        const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
+        const unsigned long long mq[4] = {m01.x, m01.y, m23.x, m23.y};
+        float sv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const double mass = static_cast<double>(mq[e]) * a.inv_scale;
+            const double rho = mass * a.inv_dx3 - a.rho_sub;
+            sv[e] = static_cast<float>(1.0 * (4.0 * kPiW * 1.0 * rho));
+        }
+        return make_float4(sv[0], sv[1], sv[2], sv[3]);
+    };
+
+    // ---- level 0 and the level before it, the source, the halo: all from global memory ----
+#pragma unroll 1
+    for (int k = 0; k < KP; ++k) {
+        const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
+        const float4 s4 = source(o4);
+        srcs[k * T + tid] = s4;
+        if (k >= 1 && k <= ZC) {
+            if (a.src != nullptr) __stcg(reinterpret_cast<float4*>(a.src) + o4, s4);
+            ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
+            const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
+            __stcg(z2 + 2 * o4, zz);
+            __stcg(z2 + 2 * o4 + 1, zz);
+        }
+    }
+    float4 cur[KP], old[KP];
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+        const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
+        cur[k] = __ldcg(c4 + o4);
+        old[k] = __ldcg(p4 + o4);
+        T4(k, r + 2)[q] = cur[k];
+    }
+    for (int i = tid; i < 4 * ZC * W; i += T) {  // rows y0-2, y0-1, y0+RB, y0+RB+1, own planes
+        const int jj = i / (ZC * W), rem = i - jj * (ZC * W), kk = rem / W, qq = rem - kk * W;
+        const int j = jj < 2 ? jj : RB + jj;
+        T4(kk + 1, j)[qq] = __ldcg(c4 + g4(z0 + kk, y0 - 2 + j) + qq);
+    }
+    for (int i = tid; i < 4 * W; i += T) {  // the four edge rows
+        const int cc = i / W, qq = i - cc * W;
+        const int j = (cc & 1) ? RB + 2 : 1, k = (cc & 2) ? KP - 1 : 0;
+        T4(k, j)[qq] = __ldcg(c4 + g4(z0 - 1 + k, y0 - 2 + j) + qq);
+    }
+    for (int i = tid; i < zhN; i += T) {  // planes z0 - 2 and z0 + ZC + 1 of the own rows
+        const int side = i / (RB * W), rem = i - side * (RB * W), rr = rem / W, qq = rem - rr * W;
+        zh[i] = __ldcg(c4 + g4(side ? z0 + ZC + 1 : z0 - 2, y0 + rr) + qq);
+    }
+    for (int i = tid; i < ringN; i += T) {  // the outer rows' previous level and source
+        const int side = i / (ZC * W), rem = i - side * (ZC * W), kk = rem / W, qq = rem - kk * W;
+        const size_t o4 = g4(z0 + kk, side ? y0 + RB : y0 - 1) + qq;
+        rold[i] = __ldcg(p4 + o4);
+        rsrc[i] = source(o4);
+    }
+    __syncthreads();
+
+    // lanes 0-7 of warp 0 watch one neighbour's counter each: y-, y+, z-, z+, then the
+    // diagonals (y-, z-), (y+, z-), (y-, z+), (y+, z+)
+    const unsigned int* watched = nullptr;
+    if (tid < 8) {
+        const int nbx = (tid == 0 || tid == 4 || tid == 6) ? bxm
+                        : (tid == 1 || tid == 5 || tid == 7) ? bxp : bx;
+        const int nbz = (tid == 2 || tid == 4 || tid == 5) ? bzm
+                        : (tid == 3 || tid == 6 || tid == 7) ? bzp : bz;
+        watched = a.sync + (nbz * gx + nbx) * kCounterStride;
+    }
+    const int nb_ym = bz * gx + bxm, nb_yp = bz * gx + bxp;
+    const int nb_zm = bzm * gx + bx, nb_zp = bzp * gx + bx;
+    const int nb_mm = bzm * gx + bxm, nb_pm = bzm * gx + bxp;
+    const int nb_mp = bzp * gx + bxm, nb_pp = bzp * gx + bxp;
+
+    // ---- pieces of a pass ------------------------------------------------------------------
+    // the block's face values of plane k (1 .. ZC) of the level of epoch e: F0 rows 0, 1;
+    // F1 rows RB - 2, RB - 1; F2 planes 1, 2; F3 planes ZC - 1, ZC
+    auto store_faces = [&](unsigned int e, int k, const float4& v) {
+        float4* const f = face(e, me);
+        if (r < 2) __stcg(f + (r * ZC + k - 1) * W + q, v);
+        else if (r >= RB - 2) __stcg(f + FY + ((r - RB + 2) * ZC + k - 1) * W + q, v);
+        if (k <= 2) __stcg(f + 2 * FY + ((k - 1) * RB + r) * W + q, v);
+        else if (k >= ZC - 1) __stcg(f + 2 * FY + FZ + ((k - ZC + 1) * RB + r) * W + q, v);
+    };
+    // substep A: level t -> t + 1 on the ten-plane columns and the outer rows; the new levels
+    // replace level t in the tile once every read of it is done. The outer rows' earlier level
+    // is read from parity par and their new one written to the other.
+    auto substep_a = [&](int par) {
+        float4 zm = zh[r * W + q];
+        const float4 ztop = zh[(RB + r) * W + q];
+#pragma unroll
+        for (int k = 0; k < KP; ++k) {
+            const float4 c = cur[k];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+            const float4 zp = k + 1 < KP ? cur[k + 1] : ztop;
+            const float4 out = wave_cell4(c, lft, rgt, T4(k, r + 1)[q], T4(k, r + 3)[q], zm, zp,
+                                          old[k], srcs[k * T + tid], km, ka, ko, kf);
+            zm = c;
+            old[k] = c;
+            cur[k] = out;
+        }
+        const int side = warp / ZC, kk = warp - side * ZC, k = kk + 1;
+        const int j = side ? RB + 2 : 1;
+        const int ri = (side * ZC + kk) * W + q;
+        float4 ring;
+        {
+            const float4 c = T4(k, j)[q];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+            ring = wave_cell4(c, lft, rgt, T4(k, j - 1)[q], T4(k, j + 1)[q], T4(k - 1, j)[q],
+                              T4(k + 1, j)[q], rold[par * ringN + ri], rsrc[ri], km, ka, ko, kf);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k2 = 0; k2 < KP; ++k2) T4(k2, r + 2)[q] = cur[k2];
+        T4(k, j)[q] = ring;
+        rold[(par ^ 1) * ringN + ri] = ring;
+        __syncthreads();
+    };
+    // substep B: the own cells (planes 1 .. ZC) one level on, from the tile and the columns'
+    // outer planes; faces stored under epoch e as they are computed
+    auto substep_b = [&](unsigned int e) {
+        float4 zm = cur[0];
+#pragma unroll
+        for (int k = 1; k <= ZC; ++k) {
+            const float4 c = cur[k];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+            const float4 out = wave_cell4(c, lft, rgt, T4(k, r + 1)[q], T4(k, r + 3)[q], zm,
+                                          cur[k + 1], old[k], srcs[k * T + tid], km, ka, ko, kf);
+            zm = c;
+            old[k] = c;
+            cur[k] = out;
+            store_faces(e, k, out);
+        }
+    };
+    // publish epoch e (the barrier orders every thread's face stores and its reads of the tile
+    // before the release), then bring in the neighbours' faces of epoch e; false for every
+    // thread when a wait ran out
+    auto exchange = [&](unsigned int e) -> bool {
+        __syncthreads();
+        if (tid == 0) st_release(counter, e);
+#pragma unroll
+        for (int k = 1; k <= ZC; ++k) T4(k, r + 2)[q] = cur[k];
+        if (tid < 8) {
+            const long long t0 = clock64();
+            for (unsigned int polls = 1; static_cast<int>(ld_acquire(watched) - e) < 0; ++polls) {
+                if (clock64() - t0 > kWaitCycles || ((polls & 255u) == 0 && *err != 0)) {
+                    fail_s = 1;
+                    atomicExch(a.sync + kErrWord, 1u);  // (the host clears it)
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        if (fail_s) return false;
+        for (int i = tid; i < HALO; i += T) {
+            const float4* from;
+            float4* to;
+            if (i < 2 * FY) {
+                // rows y0 - 2, y0 - 1 from the lower y neighbour's F1; rows y0 + RB,
+                // y0 + RB + 1 from the upper one's F0
+                const int side = i / FY, off = i - side * FY;
+                const int rr = off / (ZC * W), rem = off - rr * (ZC * W);
+                const int kk = rem / W, qq = rem - kk * W;
+                from = face(e, side ? nb_yp : nb_ym) + (side ? 0 : FY) + off;
+                to = T4(kk + 1, side ? RB + 2 + rr : rr) + qq;
+            } else if (i < 2 * FY + 2 * FZ) {
+                // planes z0 - 2, z0 - 1 from the lower z neighbour's F3; planes z0 + ZC,
+                // z0 + ZC + 1 from the upper one's F2
+                const int iz = i - 2 * FY;
+                const int side = iz / FZ, off = iz - side * FZ;
+                const int pp = off / (RB * W), rem = off - pp * (RB * W);
+                const int rr = rem / W, qq = rem - rr * W;
+                from = face(e, side ? nb_zp : nb_zm) + 2 * FY + (side ? 0 : FZ) + off;
+                if (side == 0) to = pp == 0 ? zh + rr * W + qq : T4(0, rr + 2) + qq;
+                else to = pp == 0 ? T4(KP - 1, rr + 2) + qq : zh + (RB + rr) * W + qq;
+            } else {
+                // the edge rows (y0 - 1 or y0 + RB, z0 - 1 or z0 + ZC) from the diagonal
+                // neighbours: row RB - 1 is F1's second row, row 0 F0's first; plane ZC is
+                // slot ZC - 1 of a y face, plane 1 slot 0
+                const int ic = i - 2 * FY - 2 * FZ;
+                const int cc = ic / W, qq = ic - cc * W;
+                const bool up_y = (cc & 1) != 0, up_z = (cc & 2) != 0;
+                const int nb = up_z ? (up_y ? nb_pp : nb_mp) : (up_y ? nb_pm : nb_mm);
+                const int slot = up_z ? 0 : ZC - 1;
+                from = face(e, nb) + (up_y ? slot * W : FY + (ZC + slot) * W) + qq;
+                to = T4(up_z ? KP - 1 : 0, up_y ? RB + 2 : 1) + qq;
+            }
+            cp_async16(to, from);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        // the columns' outer planes: the level before, and level t from the halo
+        old[0] = cur[0];
+        cur[0] = T4(0, r + 2)[q];
+        old[KP - 1] = cur[KP - 1];
+        cur[KP - 1] = T4(KP - 1, r + 2)[q];
+        return true;
+    };
+
+    // ---- passes of two substeps, then an odd one -------------------------------------------
+    unsigned int e = base;
+    int par = 0;
+    for (int p = 0; p < a.iterations / 2; ++p) {
+        substep_a(par);
+        par ^= 1;
+        ++e;
+        substep_b(e);
+        if (!exchange(e)) return;
+    }
+    if (a.iterations & 1) {
+        ++e;
+        substep_b(e);
+        if (!exchange(e)) return;
+    }
+
+    // ---- the levels to global memory ------------------------------------------------------
+    {
+        const bool fin0 = (a.cur ^ (a.iterations & 1)) == 0;
+        float4* fin = reinterpret_cast<float4*>(fin0 ? a.phi0 : a.phi1);
+        float4* prv = reinterpret_cast<float4*>(fin0 ? a.phi1 : a.phi0);
+#pragma unroll
+        for (int k = 1; k <= ZC; ++k) {
+            const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
+            __stcg(fin + o4, cur[k]);
+            __stcg(prv + o4, old[k]);
+        }
+    }
+
+    // ---- gradient of the final level (gradient_x4_kernel's expressions) -------------------
+    if (a.acc4 != nullptr) {
+        const int x = 4 * q, y = y0 + r;
+#pragma unroll
+        for (int k = 1; k <= ZC; ++k) {
+            const int z = z0 - 1 + k;
+            const float4 c = cur[k];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+            const float d0 = x == 0 ? c.y - c.x : 0.5f * (c.y - lft);
+            const float d1 = 0.5f * (c.z - c.x);
+            const float d2 = 0.5f * (c.w - c.y);
+            const float d3 = x + 4 == NX ? c.w - c.z : 0.5f * (rgt - c.z);
+            const float4 ym = T4(k, r + 1)[q];
+            const float4 yp = T4(k, r + 3)[q];
+            float4 ey;
+            if (y == 0) ey = make_float4(yp.x - c.x, yp.y - c.y, yp.z - c.z, yp.w - c.w);
+            else if (y == NX - 1) ey = make_float4(c.x - ym.x, c.y - ym.y, c.z - ym.z, c.w - ym.w);
+            else
+                ey = make_float4(0.5f * (yp.x - ym.x), 0.5f * (yp.y - ym.y), 0.5f * (yp.z - ym.z),
+                                 0.5f * (yp.w - ym.w));
+            const float4 zm = cur[k - 1];
+            const float4 zp = cur[k + 1];
+            float4 ez;
+            if (z == 0) ez = make_float4(zp.x - c.x, zp.y - c.y, zp.z - c.z, zp.w - c.w);
+            else if (z == NX - 1) ez = make_float4(c.x - zm.x, c.y - zm.y, c.z - zm.z, c.w - zm.w);
+            else
+                ez = make_float4(0.5f * (zp.x - zm.x), 0.5f * (zp.y - zm.y), 0.5f * (zp.z - zm.z),
+                                 0.5f * (zp.w - zm.w));
+            const float g = a.grad_coef;
+            float4* o = a.acc4 + (static_cast<size_t>(z) * NX + y) * NX + x;
+            o[0] = make_float4(d0 * g, ey.x * g, ez.x * g, c.x);
+            o[1] = make_float4(d1 * g, ey.y * g, ez.y * g, c.y);
+            o[2] = make_float4(d2 * g, ey.z * g, ez.z * g, c.z);
+            o[3] = make_float4(d3 * g, ey.w * g, ez.w * g, c.w);
+        }
+    }
+    // the counter ends at base + (passes) in every block: the next launch starts from there
+}
+
+bool use_tb() {
+    // RRG_WAVE_TB=0 keeps the one-exchange-per-substep kernel on 128^3 (same bits); read once per
+    // process, since the two kernels lay out the synchronisation memory differently
+    static const bool on = [] {
+        const char* e = std::getenv("RRG_WAVE_TB");
+        return !(e && std::atoi(e) == 0);
+    }();
+    return on;
+}
+
 template <int W>
 void set_smem_attr() {
     RRG_CUDA(cudaFuncSetAttribute(wave_solve_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -372,7 +739,8 @@ bool wave_solve_applicable(int nx) {
 }
 
 size_t wave_solve_sync_bytes(int nx) {
-    return (nx == 32 || nx == 64 || nx == 128) ? sync_bytes_for(block_count(nx)) : kFaceOffset;
+    if (nx == 128) return std::max(sync_bytes_for(block_count(nx)), sync_bytes_tb(128));
+    return (nx == 32 || nx == 64) ? sync_bytes_for(block_count(nx)) : kFaceOffset;
 }
 
 bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur,
@@ -380,10 +748,12 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
                        double dx, double rho_sub, const WaveCoef& w, float* src, float4* acc4,
                        unsigned int* sync, size_t sync_bytes, cudaStream_t s) {
     if (!wave_solve_applicable(nx) || iterations < 1) return false;
-    const int W = nx / 4, RB = kThreads / W;
+    const bool tbk = nx == 128 && use_tb();
+    const int W = nx / 4, RB = (tbk ? tb::T : kThreads) / W;
     const dim3 grid(nx / RB, nx / kZC);
     const int64_t nblocks = static_cast<int64_t>(grid.x) * grid.y;
-    RRG_REQUIRE(nblocks * kCounterStride < kErrWord && sync_bytes >= sync_bytes_for(nblocks),
+    RRG_REQUIRE(nblocks * kCounterStride < kErrWord &&
+                    sync_bytes >= (tbk ? sync_bytes_tb(nblocks) : sync_bytes_for(nblocks)),
                 RRG_ERR_INVALID, "wave solve: sync memory too small for the grid");
     int dev = 0;
     RRG_CUDA(cudaGetDevice(&dev));
@@ -396,11 +766,18 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
             set_smem_attr<8>();
             set_smem_attr<16>();
             set_smem_attr<32>();
+            RRG_CUDA(cudaFuncSetAttribute(wave_solve_tb_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(tb::smem)));
             if (dev >= 0 && dev < 64) done[dev] = true;
         }
     }
-    const int per_sm = W == 8 ? blocks_per_sm<8>()
-                              : (W == 16 ? blocks_per_sm<16>() : blocks_per_sm<32>());
+    int per_sm = 0;
+    if (tbk)
+        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_solve_tb_kernel,
+                                                               tb::T, tb::smem));
+    else
+        per_sm = W == 8 ? blocks_per_sm<8>() : (W == 16 ? blocks_per_sm<16>() : blocks_per_sm<32>());
     if (static_cast<int64_t>(per_sm) * num_sms(dev) < nblocks)
         return false;  // not all blocks could be resident at once
     SolveArgs a;
@@ -430,7 +807,11 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (W == 8) {
+    if (tbk) {
+        cfg.blockDim = dim3(tb::T);
+        cfg.dynamicSmemBytes = tb::smem;
+        RRG_CUDA(cudaLaunchKernelEx(&cfg, wave_solve_tb_kernel, a));
+    } else if (W == 8) {
         cfg.dynamicSmemBytes = Shape<8>::smem;
         RRG_CUDA(cudaLaunchKernelEx(&cfg, wave_solve_kernel<8>, a));
     } else if (W == 16) {

@@ -167,6 +167,17 @@ def test_generators_deterministic_and_shaped():
     assert abs(np.median(np.abs(pd[:, 2])) - 0.1 * np.arctanh(0.5)) < 0.01
 
 
+def test_oracle_disk_generator_gives_the_library_bits():
+    """The timed CPU arm of the benchmark makes its inputs with the oracle's restatement of the
+    disk generator (so it loads nothing of the product): the same bits for the same seed."""
+    import oracle as orc
+    for seed, n in ((1, 30000), (7, 1000)):
+        po, vo = orc.exp_disk(seed, n, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1)
+        pl, vl = rg.generate_exp_disk(seed, n, 1.0, 1.0, 0.1, 7.5, 7.5, 0.1)
+        np.testing.assert_array_equal(po, pl)
+        np.testing.assert_array_equal(vo, vl)
+
+
 @pytest.mark.parametrize("fault", ["no_params", "bad_json", "missing_ic", "truncated_ic",
                                    "short_row"])
 def test_rrgsim_executable_reports_host_faults(tmp_path, fault):

@@ -215,9 +215,11 @@ def test_asynchronous_conservation_sums_equal_the_synchronous_ones(memory):
         np.testing.assert_array_equal(got["angular"], ref["angular"])
 
 
-def test_raw_device_entry_points_match_context():
+@pytest.mark.parametrize("n", [3000, 3001, 65537])
+def test_raw_device_entry_points_match_context(n):
+    # n = 3001 and 65537 (n % 4 != 0, several j-splits): the split partials must still start
+    # on a 16-byte boundary behind the n-float potential
     torch = pytest.importorskip("torch")
-    n = 3000
     pos, vel, m, s2 = plummer(n, seed=8)
     posm = torch.tensor(np.hstack([pos, m[:, None]]), dtype=torch.float32, device="cuda")
     out = torch.empty((n, 4), dtype=torch.float32, device="cuda")

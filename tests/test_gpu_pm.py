@@ -331,7 +331,7 @@ def test_step_by_step_calls_equal_one_long_call(prec, interval):
     sim = rg.SimParams(time_max=1.0, dt_save=0.1, dt_dynamics=dt, saves_without_dump=2 ** 63,
                        use_wave_model=1)
     out = []
-    for plan in ("long", "single", "split"):
+    for plan in ("long", "single", "split", "prepared"):
         with _ctx(prec, pos, vel, m, s2, g) as c:
             c.set_sort_interval(interval)
             c.set_wave_params(wp)
@@ -342,6 +342,18 @@ def test_step_by_step_calls_equal_one_long_call(prec, interval):
             elif plan == "single":
                 for _ in range(12):
                     c.calc_steps(1)
+            elif plan == "prepared":
+                # recording the graphs of the next call ahead of it runs nothing and changes
+                # nothing
+                c.calc_steps(3)
+                before = c.get_particles()
+                c.prepare_steps(9)
+                c.prepare_steps(9)
+                after = c.get_particles()
+                for k in ("pos", "vel", "acc"):
+                    np.testing.assert_array_equal(before[k], after[k])
+                assert c.time()[1] == 3
+                c.calc_steps(9)
             else:
                 c.calc_steps(5)
                 mid = c.get_particles()
@@ -367,7 +379,8 @@ def test_step_by_step_calls_equal_one_long_call(prec, interval):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
-@pytest.mark.parametrize("nx,iterations", [(32, 20), (64, 7), (64, 1), (128, 20)])
+@pytest.mark.parametrize("nx,iterations", [(32, 20), (64, 7), (64, 1), (128, 20), (128, 7),
+                                           (128, 1)])
 def test_persistent_wave_solve_equals_one_launch_per_substep(monkeypatch, prec, nx, iterations):
     """Periodic FP32 grids of 32, 64 and 128 cells run each step's source, substeps and
     gradient as one persistent kernel; RRG_WAVE_PERSIST=0 launches them one by one. Same bits
@@ -411,10 +424,11 @@ def test_persistent_wave_solve_equals_one_launch_per_substep(monkeypatch, prec, 
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
-@pytest.mark.parametrize("nx", [64, 40])
+@pytest.mark.parametrize("nx", [64, 40, 128])
 def test_solve_wave_and_field_equals_separate_calls(prec, nx):
-    """The one-call solve (the persistent kernel on FP32 / MIXED 64^3; separate launches on
-    40^3 and in FP64) leaves the same bits as solve_wave_equation + calc_acceleration_field."""
+    """The one-call solve (the persistent kernels on FP32 / MIXED 64^3 and 128^3; separate
+    launches on 40^3 and in FP64) leaves the same bits as solve_wave_equation +
+    calc_acceleration_field."""
     pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, prec)
     wp.steady_check_step = 10 ** 6  # no steady checks inside the 7 substeps
     out = []
@@ -438,14 +452,15 @@ def test_solve_wave_and_field_equals_separate_calls(prec, nx):
         np.testing.assert_array_equal(a, b)
 
 
-def test_persistent_solve_reports_a_wait_that_ran_out():
+@pytest.mark.parametrize("nx", [64, 128])
+def test_persistent_solve_reports_a_wait_that_ran_out(nx):
     """Every wait between the persistent solve's thread blocks is bounded (~0.14 s). Rewinding
     one block's epoch counter makes its neighbours wait for epochs it never publishes: the
     waits run out, the kernel sets its error word and returns, the next synchronising call
-    raises, and after that the context computes the same bits as a fresh one."""
+    raises, and after that the context computes the same bits as a fresh one. (128^3 runs the
+    two-substeps-per-exchange kernel, 64^3 the one-exchange-per-substep kernel.)"""
     from cuda.bindings import runtime as cudart
 
-    nx = 64
     pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, "fp32")
 
     def fresh_solve(c):
@@ -473,3 +488,41 @@ def test_persistent_solve_reports_a_wait_that_ran_out():
         got = fresh_solve(c)
     for k in want:
         np.testing.assert_array_equal(got[k], want[k])
+
+
+def test_load_particles_rejects_bad_input_on_the_device():
+    """The upload is checked on the device: the lowest offending particle is named, positions
+    and velocities before masses before softenings, and the context keeps its particles."""
+    pos, vel, m, s2 = disk(5000, seed=4)
+    g = _grid(16)
+    with _ctx("fp32", pos, vel, m, s2, g) as c:
+        keep = c.get_particles()
+        cases = []
+        p = pos.copy()
+        p[1234, 1] = np.nan
+        v = vel.copy()
+        v[3000, 2] = np.inf
+        cases.append(((p, v, m, s2), "non-finite position/velocity at particle 1234"))
+        mm = m.copy()
+        mm[77] = -1.0
+        ss = s2.copy()
+        ss[77] = np.nan
+        cases.append(((pos, vel, mm, ss), "bad mass at particle 77"))
+        ss = s2.copy()
+        ss[4999] = -1e-4
+        cases.append(((pos, vel, m, ss), "bad soft2 at particle 4999"))
+        for args, msg in cases:
+            with pytest.raises(rg.RRGError) as e:
+                c.load_particles(*args)
+            assert msg in str(e.value)
+        got = c.get_particles()
+        for k in ("pos", "vel"):
+            np.testing.assert_array_equal(got[k], keep[k])
+        # uniform and non-uniform masses / softenings both load
+        mm = m.copy()
+        mm[::3] *= 2.0
+        ss = s2.copy()
+        ss[::2] = 4e-4
+        c.load_particles(pos, vel, mm, ss)
+        c.convert_particles_to_grid()
+        assert abs(c.get_grid()["mass"].sum() - f32(mm).sum()) <= 1e-6 * mm.sum()

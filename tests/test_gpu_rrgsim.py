@@ -9,7 +9,7 @@ import pytest
 
 import oracle as orc
 import rrgsim_b200 as rg
-from helpers import disk, plummer, rel_err
+from helpers import disk, f32, plummer, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -74,6 +74,70 @@ def test_rrgsim_nbody_dumps_match_oracle(tmp_path):
     assert any((tmp_path / "logs").iterdir())
 
 
+def _table(path):
+    rows = path.read_text().splitlines()
+    head = [h.strip() for h in rows[0].split(",")]
+    vals = np.array([[float(x) for x in r.split(",")] for r in rows[1:]])
+    return head, vals
+
+
+def test_rrgsim_tables_follow_the_reference_formulas(tmp_path):
+    """The conservation and sample tables (print_conservation, print_sample_particle:
+    rrgsim_conservation.cu:9-98, 334-359) recomputed from the dumped snapshots with the FP64
+    oracle: E = Ek + Ep with Ep = sum m phi / 2, |P|, L_z and |L|, each with its relative change
+    against the start; the sample row is particle 0."""
+    n, dt = 512, 1e-3
+    pos, vel, m, s2 = plummer(n, seed=23)
+    _write_case(tmp_path, pos, vel, {"time_max": 0.02, "dt_save": 0.005, "dt_dynamics": dt,
+                                     "saves_without_dump": 3})
+    _run(tmp_path)
+    data = tmp_path / "data"
+
+    def cons(p, v):
+        c = orc.conservation(p, v, m, orc.direct_grav(p, m, s2))
+        L = c["angular"]
+        return {"E": c["Ek"] + c["Ep"], "Ek": c["Ek"], "Ep": c["Ep"],
+                "P": np.linalg.norm(c["momentum"]), "Lz": L[2], "L": np.linalg.norm(L)}
+
+    c0 = cons(f32(pos), f32(vel))
+    he, te = _table(data / "delta_energy.csv")
+    hp, tp = _table(data / "delta_momentum.csv")
+    hz, tz = _table(data / "delta_ang_z.csv")
+    hn, tn = _table(data / "delta_ang_norm.csv")
+    hs, ts = _table(data / "sample_particle.csv")
+    assert hp == ["t", "momentum_norm", "momentum_diff", "momentum_rel_signed", "momentum_rel"]
+    assert hz == ["t", "ang_z", "ang_z_rel_signed", "ang_z_rel"]
+    assert hn == ["t", "ang_norm", "ang_norm_rel_signed", "ang_norm_rel"]
+    assert hs == ["i", "x", "y", "z", "vx", "vy", "vz", "grav", "ax", "ay", "az"]
+    assert len(ts) == 1 + 4  # the start, then every save
+    for row, name in ((0, "S_    5.bin"), (1, "S_   10.bin")):
+        t, dp, dv = _read_dump(tmp_path / "dump" / name)
+        c = cons(dp, dv)
+        e_rel = c["E"] / c0["E"] - 1
+        assert abs(te[row, 0] - t) < 1e-8
+        np.testing.assert_allclose(te[row, [1, 4, 5]], [c["E"], c["Ek"], c["Ep"]], rtol=1e-5)
+        assert abs(te[row, 2] - e_rel) < 5e-6 and abs(te[row, 3] - abs(e_rel)) < 5e-6
+        p_rel = c["P"] / c0["P"] - 1
+        np.testing.assert_allclose(tp[row, 1], c["P"], rtol=1e-9)
+        np.testing.assert_allclose(tp[row, 2], c["P"] - c0["P"], atol=1e-12)
+        assert abs(tp[row, 3] - p_rel) < 1e-8 and abs(tp[row, 4] - abs(p_rel)) < 1e-8
+        lz_rel = c["Lz"] / c0["Lz"] - 1
+        np.testing.assert_allclose(tz[row, 1], c["Lz"], rtol=1e-9)
+        assert abs(tz[row, 2] - lz_rel) < 1e-8 and abs(tz[row, 3] - abs(lz_rel)) < 1e-8
+        ln_rel = c["L"] / c0["L"] - 1
+        np.testing.assert_allclose(tn[row, 1], c["L"], rtol=1e-9)
+        assert abs(tn[row, 2] - ln_rel) < 1e-8
+        # sample particle: index 0 at this save, 8 decimals
+        s = ts[row + 1]
+        assert s[0] == 0
+        np.testing.assert_allclose(s[1:4], dp[0], atol=1e-8)
+        np.testing.assert_allclose(s[4:7], dv[0], atol=1e-8)
+        np.testing.assert_allclose(s[7], orc.direct_grav(dp, m, s2)[0], rtol=1e-5, atol=1e-7)
+        np.testing.assert_allclose(s[8:11], orc.direct_acc(dp, m, s2)[0], rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(ts[0, 1:4], f32(pos)[0], atol=1e-8)
+    np.testing.assert_allclose(ts[0, 4:7], f32(vel)[0], atol=1e-8)
+
+
 def test_rrgsim_wave_mode_runs_and_matches_library(tmp_path):
     n, nx, dt = 4096, 16, 2e-3
     pos, vel, m, s2 = disk(n, seed=22)
@@ -103,11 +167,29 @@ def test_rrgsim_wave_mode_runs_and_matches_library(tmp_path):
         ctx.sync_particles_and_grid()
         ctx.calc_steps(2)
         s = ctx.get_particles()
+        gr = ctx.get_grid()
     t, dp, dv = _read_dump(tmp_path / "dump" / "S_    2.bin")
     np.testing.assert_array_equal(dp, s["pos"])
     np.testing.assert_array_equal(dv, s["vel"])
     for sub in ("a_grid", "grav_grid", "mass_grid"):
         assert any((tmp_path / "data" / sub).iterdir())
+    # the axis profiles through the centre at t = 2 dt (print_acc_projection and friends,
+    # rrgsim_conservation.cu:360-424), 8 decimals, against the library's grid at that step
+    h = nx // 2
+    at = lambda x, y, z: x + y * nx + z * nx * nx  # noqa: E731
+    xs = -0.5 * nx * dx + dx * np.arange(nx)
+    ha, ta = _table(tmp_path / "data" / "a_grid" / "a_grid_center_0.00400000.csv")
+    assert ha == ["x", "ax", "ay", "az"]
+    np.testing.assert_allclose(ta[:, 0], xs, atol=1e-8)
+    np.testing.assert_allclose(ta[:, 1:], gr["acc"][[at(i, h, h) for i in range(nx)]], atol=1e-8)
+    hg, tg = _table(tmp_path / "data" / "grav_grid" / "grav_axis_center_0.0040000000.csv")
+    assert hg == ["r", "gx", "gy", "gz"]
+    for col, idx in ((1, [at(i, h, h) for i in range(nx)]), (2, [at(h, i, h) for i in range(nx)]),
+                     (3, [at(h, h, i) for i in range(nx)])):
+        np.testing.assert_allclose(tg[:, col], gr["grav"][idx], atol=1e-8)
+    hm, tm = _table(tmp_path / "data" / "mass_grid" / "mass_axis_center_0.0040000000.csv")
+    assert hm == ["r", "mx", "my", "mz"]
+    np.testing.assert_allclose(tm[:, 1], gr["mass"][[at(i, h, h) for i in range(nx)]], atol=1e-8)
 
 
 @pytest.mark.parametrize("mode,precision", [("nbody", "fp32"), ("wave", "fp32"),

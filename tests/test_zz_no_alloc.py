@@ -10,6 +10,7 @@ last so a failure here cannot hide the result of any other test.
 import numpy as np
 import pytest
 
+import oracle as orc
 import rrgsim_b200 as rg
 from helpers import plummer
 
@@ -20,7 +21,7 @@ def _posm(torch, pos, m):
     return torch.tensor(np.hstack([pos, m[:, None]]), dtype=torch.float32, device="cuda")
 
 
-@pytest.mark.parametrize("n", [1, 3000, 4096, 65536])
+@pytest.mark.parametrize("n", [1, 3000, 3001, 4096, 65536, 65537])
 def test_noalloc_matches_allocating_entry_point(n):
     torch = pytest.importorskip("torch")
     L = rg.lib()
@@ -45,6 +46,11 @@ def test_noalloc_matches_allocating_entry_point(n):
         # same kernels; only the number of j-splits may differ, so the FP32 sums may differ
         # in the last bits: hold them to the direct-sum FP32 tolerance
         np.testing.assert_allclose(o, r, rtol=1e-5, atol=1e-6 * np.abs(r).max())
+        # and against the FP64 oracle: the direct sum's median relative error bar
+        if 2 <= n <= 4096:  # (n = 1: the self pair alone, zero force)
+            acc = orc.direct_acc(pos, m, s2)
+            err = np.linalg.norm(o[:, :3] - acc, axis=1) / np.linalg.norm(acc, axis=1)
+            assert np.median(err) <= 1e-5
 
 
 def test_noalloc_with_per_particle_softening():

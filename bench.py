@@ -177,6 +177,20 @@ def pm_step_error(ctx, mass, grid, wave) -> dict:
             "pos_rel_median": float(np.median(ep)), "pos_rel_max": float(np.max(ep))}
 
 
+def direct_errors(c3: dict) -> dict:
+    """Median and 99th-percentile relative error of the bulge + disk initial accelerations in
+    each precision against the FP64 oracle's direct sum of the same inputs."""
+    import oracle as orc
+    pos, m, s2 = c3.pop("inputs")
+    orc.set_threads(os.cpu_count() or 1)
+    ref = orc.direct_acc(pos, m, s2)
+    out = {}
+    for prec, acc in c3.pop("acc0").items():
+        e = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        out[prec] = {"median": float(np.median(e)), "p99": float(np.percentile(e, 99))}
+    return out
+
+
 def cpu_pm_sample(state, steps: int, threads: int) -> tuple[float, str]:
     """Times `steps` PM steps of the CPU restatement (FP64, OpenMP) at full size from the given
     relaxed state; returns (particle-steps/s, sample description)."""
@@ -292,9 +306,6 @@ def run_native(args):
     barrier(world)
     el = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
     value = N_PART * args.steps * world / el
-
-    # ---- the error of one fused step against the FP64 oracle, outside the timed region ------
-    error = pm_step_error(ctx, mass, grid, wave) if rank == 0 else None
 
     # ---- dominant kernel: the persistent wave solve (source, 20 substeps, gradient in one
     # launch), timed alone on the same stream with L2 flushed before every launch ------------------
@@ -438,9 +449,20 @@ def run_native(args):
                   "fp32_peak_tflops": fp32_peak, "fp32_peak_kind": "nominal at sm_max_mhz"}
         cd.close()
 
-    # ---- CPU baseline (rank 0, bounded sample) -------------------------------------------------
-    cpu = None
+    # ---- the secondary forms in brief (rank 0, one GPU) ---------------------------------------
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        from rrgsim_b200.bench_forms import bench_line_forms
+        forms = bench_line_forms(torch)
+
+    # ---- CPU leg (rank 0): the oracle checks one fused step of the workload and the forms'
+    # accelerations, then times a bounded sample of the workload ---------------------------------
+    cpu = error = None
     if rank == 0 and not args.no_cpu:
+        error = pm_step_error(ctx, mass, grid, wave)
+        if forms is not None:
+            forms["precision_c3"]["acc_rel_err_vs_fp64_oracle"] = direct_errors(
+                forms["precision_c3"])
         part = ctx.get_particles()
         g = ctx.get_grid()
         # the CPU restatement starts from the GPU's relaxed potential (both levels)
@@ -449,6 +471,9 @@ def run_native(args):
         v_cpu, sample = cpu_pm_sample(state, args.cpu_steps, threads)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": sample}
+    if forms is not None:  # (arrays the CPU leg did not take)
+        forms["precision_c3"].pop("inputs", None)
+        forms["precision_c3"].pop("acc0", None)
     ctx.close()
 
     if rank == 0:
@@ -484,6 +509,7 @@ def run_native(args):
             "error_vs_fp64": error,
             "clocks": clk,
             "direct_sum": direct,
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -499,6 +525,8 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the secondary forms (precision, ensemble, adjoint)")
     ap.add_argument("--sort-interval", type=int, default=None,
                     help="steps between re-sorts of the particles by cell (default: the library's)")
     ap.add_argument("--setup-iterations", type=int, default=20000,

@@ -5,11 +5,13 @@
 # Output only into oracle/_ref/ (git-ignored; it travels to the GPU box with the tree).
 # Test infrastructure only: nothing in the product links it.
 set -euo pipefail
-REF=${RRG_REFERENCE:-/root/reference}
+# RRG_REFERENCE: the reference project's root (the directory holding solver/); without it the
+# prebuilt library, if any, is kept
+REF=${RRG_REFERENCE:-}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 NVCC=${NVCC:-nvcc}
-if [ ! -d "$REF/solver" ]; then
+if [ -z "$REF" ] || [ ! -d "$REF/solver" ]; then
   echo "reference sources not found at $REF; keeping any prebuilt $OUT/librrgref.so" >&2
   exit 0
 fi

@@ -251,7 +251,7 @@ def bench_form(torch_mod=None, n=16384, nsteps=200, dt=1e-3, eps=0.02, every=20,
                        mr.grad.double().cpu().numpy())
         res[prec] = {"forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
                      "loss": float(loss.detach())}
-        if prec == "fp64":
+        if prec == "fp64" and fd_dirs > 0:
             # central differences along random directions in (x0, v0, m), FP64 forward model
             fd_rel = []
             gvec = np.concatenate([g.ravel() for g in grads["fp64"]])
@@ -425,7 +425,7 @@ def bench_form_pm(torch_mod=None, n=262144, nx=64, nsteps=200, dt=2e-3, substeps
         grads[prec] = np.concatenate([a.grad.double().cpu().numpy().ravel() for a in (xr, vr, mr)])
         res[prec] = {"forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
                      "loss": float(loss.detach())}
-        if prec == "fp64":
+        if prec == "fp64" and fd_dirs > 0:
             h = 1e-3
             rel, rel32 = [], []
             with torch.no_grad():

@@ -193,6 +193,53 @@ def form_ensemble(torch, steps=500):
             "tuning": res["batched"]["tuning"]}
 
 
+def bench_line_forms(torch, precision_steps=1000, ensemble_steps=50):
+    """The secondary forms in brief, for the benchmark's JSON line (about half a minute):
+    c3: the bulge + disk N = 65,536 in FP32, MIXED and FP64 (initial accelerations returned as
+        arrays for the caller's error check; energy drift over `precision_steps` steps);
+    c4: the 64-galaxy ensemble batched against 64 sequential launches;
+    c5: adjoint / forward wall time, N-body and particle mesh (no finite differences)."""
+    from . import adjoint
+    t0 = time.perf_counter()
+    n, dt = 65536, 1e-3
+    pos, vel, m, s2 = _bulge_disk(n)
+    sim = rg.SimParams(time_max=10.0, dt_save=1.0, dt_dynamics=dt, saves_without_dump=0,
+                       use_wave_model=0)
+    s = torch.cuda.Stream()
+    c3 = {"particles": n, "steps": precision_steps, "dt": dt, "acc0": {}}
+    for prec in ("fp32", "mixed", "fp64"):
+        with rg.Context(0, prec) as c:
+            c.set_stream(s.cuda_stream)
+            c.load_particles(pos, vel, m, s2)
+            c.solver_init(sim)
+            c.precalc()
+            c3["acc0"][prec] = c.get_particles()["acc"]
+            if prec == "fp64":
+                continue
+            e0 = c.calc_conservation()
+            a, b = _events(torch, s)
+            c.prepare_steps(precision_steps)
+            a.record(s)
+            c.calc_steps(precision_steps)
+            b.record(s)
+            torch.cuda.synchronize()
+            c.sync_particles_and_grid()
+            e1 = c.calc_conservation()
+            c3[prec] = {"energy_drift": (e1["Ek"] + e1["Ep"]) / (e0["Ek"] + e0["Ep"]) - 1.0,
+                        "gpairs_per_s": n * n * precision_steps /
+                        (a.elapsed_time(b) * 1e-3) / 1e9}
+    c3["inputs"] = (pos, m, s2)
+    c4 = form_ensemble(torch, steps=ensemble_steps)
+    c4.pop("tuning", None)
+    an = adjoint.bench_form(fd_dirs=0)
+    ap = adjoint.bench_form_pm(fd_dirs=0)
+    c5 = {"nbody_16384_200_steps": {p: an[p]["backward_over_forward"] for p in ("fp32", "fp64")},
+          "pm_262144_64_200_steps": {p: ap[p]["backward_over_forward"] for p in ("fp32", "fp64")},
+          "target": "<= 3"}
+    return {"precision_c3": c3, "ensemble_c4": c4, "adjoint_c5": c5,
+            "seconds": time.perf_counter() - t0}
+
+
 def main(argv):
     import torch
     which = argv[1] if len(argv) > 1 else "all"

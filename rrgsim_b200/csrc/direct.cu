@@ -489,7 +489,8 @@ void dispatch_f32(bool usoft, bool mixed, bool pot, dim3 grid, const F32Params& 
 }
 
 // Kernel variants of the FP32 path: 1 = scalar, 1 i per thread; 2 = scalar, 2 i per thread;
-// 3 = paired f32x2, 2 i per thread; 4 = paired f32x2, 4 i per thread. MIXED and FP64 use the
+// 3 = paired f32x2, 2 i per thread; 4 = paired f32x2, 4 i per thread; 5 = paired f32x2, 6 i
+// per thread. MIXED and FP64 use the
 // scalar kernels. RRG_DIRECT_VARIANT overrides the choice (for sweeps).
 int env_variant() {
     static const int v = [] {
@@ -503,19 +504,19 @@ int variant_for(int prec, int64_t n) {
     if (prec == RRG_PREC_FP64) return 1;
     const int e = env_variant();
     if (prec == RRG_PREC_MIXED) return (e == 1 || e == 2) ? e : (n <= 16384 ? 1 : 2);
-    if (e >= 1 && e <= 4) return e;
+    if (e >= 1 && e <= 5) return e;
     // measured on B200 (Plummer, FP32): the paired kernels lead from N = 16k on; 4 i-particles
     // per thread pay off once there are enough blocks to fill the machine
     return n < 131072 ? 3 : 4;
 }
 
-int ipt_of(int variant) { return variant == 1 ? 1 : variant == 4 ? 4 : 2; }
+int ipt_of(int variant) { return variant == 1 ? 1 : variant == 4 ? 4 : variant == 5 ? 6 : 2; }
 
 int ipt_for(int prec, int64_t n) { return ipt_of(variant_for(prec, n)); }
 
 // Resident 256-thread blocks per SM of the kernel a variant launches (queried once).
 int resident_blocks(int prec, int variant) {
-    static int cache[3][5] = {};
+    static int cache[3][6] = {};
     int& r = cache[prec][variant];
     if (r) return r;
     const void* k = nullptr;
@@ -526,7 +527,8 @@ int resident_blocks(int prec, int variant) {
     else if (variant == 1) k = reinterpret_cast<const void*>(&direct_f32_kernel<1, true, false, false>);
     else if (variant == 2) k = reinterpret_cast<const void*>(&direct_f32_kernel<2, true, false, false>);
     else if (variant == 3) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<1, true, false, false>);
-    else k = reinterpret_cast<const void*>(&direct_f32x2_kernel<2, true, false, false>);
+    else if (variant == 4) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<2, true, false, false>);
+    else k = reinterpret_cast<const void*>(&direct_f32x2_kernel<3, true, false, false>);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kBS, 0) != cudaSuccess || nb < 1) {
         (void)cudaGetLastError();
@@ -583,7 +585,7 @@ void launch_direct(const DirectLaunch& L) {
     RRG_REQUIRE(real_splits <= 1 || (reinterpret_cast<uintptr_t>(L.scratch) & 15u) == 0,
                 RRG_ERR_INVALID, "direct sum: split partials must start on a 16-byte boundary");
     const bool usoft = (L.hsoft == nullptr);
-    const int variant = (L.prec == RRG_PREC_FP32 && L.variant >= 1 && L.variant <= 4)
+    const int variant = (L.prec == RRG_PREC_FP32 && L.variant >= 1 && L.variant <= 5)
                             ? L.variant
                             : variant_for(L.prec, L.n);
     const int ipt = L.prec == RRG_PREC_FP64 ? 1 : ipt_of(variant);
@@ -647,9 +649,12 @@ void launch_direct(const DirectLaunch& L) {
         if (variant == 3) {
             if (umass) RRG_X2M(1, true);
             else RRG_X2M(1, false);
-        } else {
+        } else if (variant == 4) {
             if (umass) RRG_X2M(2, true);
             else RRG_X2M(2, false);
+        } else {
+            if (umass) RRG_X2M(3, true);
+            else RRG_X2M(3, false);
         }
 #undef RRG_X2M
     } else if (ipt == 1) {

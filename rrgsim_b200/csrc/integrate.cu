@@ -117,21 +117,40 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
     Casc acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = Casc{0.0, 0.0};
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const V4<R> p = posm[i];
+    // the next particle's loads are issued before this one's sums (a thread's FP64 chains
+    // would otherwise wait out a memory latency per particle)
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    V4<R> pn{}, vn{};
+    V4<float> ln{};
+    R phn = R(0);
+    if (i < n) {
+        pn = posm[i];
+        vn = vel[i];
+        if constexpr (MIXED) ln = lo[i];
+        if (pot) phn = pot[i];
+    }
+    for (; i < n; i += stride) {
+        const V4<R> p = pn, v = vn;
+        const V4<float> l = ln;
+        const R ph = phn;
+        const int64_t i2 = i + stride;
+        if (i2 < n) {
+            pn = posm[i2];
+            vn = vel[i2];
+            if constexpr (MIXED) ln = lo[i2];
+            if (pot) phn = pot[i2];
+        }
         double x = p.x, y = p.y, z = p.z;
         if constexpr (MIXED) {
-            const V4<float> l = lo[i];
             x += l.x;
             y += l.y;
             z += l.z;
         }
         const double m = p.w;
-        const V4<R> v = vel[i];
         const double vx = v.x, vy = v.y, vz = v.z;
         casc_add(acc[0], m * (vx * vx + vy * vy + vz * vz));
-        casc_add(acc[1], pot ? m * static_cast<double>(pot[i]) : 0.0);
+        casc_add(acc[1], pot ? m * static_cast<double>(ph) : 0.0);
         casc_add(acc[2], m * vx);
         casc_add(acc[3], m * vy);
         casc_add(acc[4], m * vz);

@@ -104,17 +104,33 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
     const unsigned heads0 = __ballot_sync(0xffffffffu, lane == 0 || below0 != key);
     if (__popc(heads0) > 4) {  // warp-uniform
         int src = lane;
+        if (nx <= 406) {
+            // (cell + 1, lane) packed into one int (nx^3 < 2^26): one shuffle per step
+            int kv = ((key + 1) << 5) | lane;
 #pragma unroll
-        for (int k = 2; k <= 32; k <<= 1) {
+            for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                const int pk = __shfl_xor_sync(0xffffffffu, key, j);
-                const int ps = __shfl_xor_sync(0xffffffffu, src, j);
-                const bool ascending = (lane & k) == 0, lower = (lane & j) == 0;
-                const bool less = pk < key || (pk == key && ps < src);
-                if (lower == ascending ? less : !less) {
-                    key = pk;
-                    src = ps;
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const int pk = __shfl_xor_sync(0xffffffffu, kv, j);
+                    const bool ascending = (lane & k) == 0, lower = (lane & j) == 0;
+                    if (lower == ascending ? pk < kv : pk > kv) kv = pk;
+                }
+            }
+            key = (kv >> 5) - 1;
+            src = kv & 31;
+        } else {
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const int pk = __shfl_xor_sync(0xffffffffu, key, j);
+                    const int ps = __shfl_xor_sync(0xffffffffu, src, j);
+                    const bool ascending = (lane & k) == 0, lower = (lane & j) == 0;
+                    const bool less = pk < key || (pk == key && ps < src);
+                    if (lower == ascending ? less : !less) {
+                        key = pk;
+                        src = ps;
+                    }
                 }
             }
         }

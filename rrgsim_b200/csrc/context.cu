@@ -286,6 +286,43 @@ bool solve_step_persistent(rrg_ctx* c, const WaveCoef& w, int iterations, bool s
     return true;
 }
 
+// The same solve one launch per substep, where the persistent kernel does not apply (grid
+// size, RRG_WAVE_PERSIST=0, residency) on FP32 / MIXED periodic grids without an absorbing
+// layer: the incremental form (wave_inc_source), the same bits as the persistent kernel. The
+// increments and their source live in the field buffer (acc4: 4 floats per cell), which the
+// gradient rewrites at the end. False (nothing launched) on other grids.
+bool solve_step_incremental(rrg_ctx* c, const WaveCoef& w, int iterations, bool store_src) {
+    if (c->prec == RRG_PREC_FP64 || c->bc_type != RRG_BC_PERIODIC || c->keep_layer) return false;
+    const int nx = c->grid.nx;
+    const size_t nc = static_cast<size_t>(nx) * nx * nx;
+    float* a4 = c->acc4.as<float>();
+    float* d[2] = {a4, a4 + nc};
+    float* g = a4 + 2 * nc;
+    float* phi0 = c->phi[c->phi_cur].as<float>();
+    float* prev = c->phi[1 - c->phi_cur].as<float>();
+    if (store_src) wave_source(c, false);
+    launch_wave_inc_prep(nx, c->mg[c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
+                         c->rho_mean, phi0, prev, w, g, d[0], d[1], c->stream);
+    // the persistent kernel clears the next deposit target too
+    RRG_CUDA(cudaMemsetAsync(c->mg[1 - c->mg_cur].p, 0, c->mg[1 - c->mg_cur].bytes, c->stream));
+    WaveCoef wi = w;
+    wi.K_F = 1.0;
+    int cur = 0;
+    for (int k = 0; k < iterations; ++k) {
+        launch_wave_step(c->prec, nx, d[cur], d[1 - cur], g, wi, nullptr, c->stream);
+        cur = 1 - cur;
+    }
+    // final level into phi[phi_cur ^ (iterations & 1)], the one before into the other
+    float* fin = c->phi[c->phi_cur ^ (iterations & 1)].as<float>();
+    float* prv = c->phi[1 - (c->phi_cur ^ (iterations & 1))].as<float>();
+    launch_wave_inc_finish(nx, phi0, d[cur], d[1 - cur], fin, prv, c->stream);
+    if (iterations % 2 == 1) c->phi_cur = 1 - c->phi_cur;
+    gradient(c);
+    c->src_dirty = false;
+    c->src_valid = store_src;
+    return true;
+}
+
 // After a synchronisation: the persistent solve's error word is set when a wait between its
 // thread blocks ran out, which leaves the steps since the last check invalid.
 void check_wave_solve(rrg_ctx* c) {
@@ -489,7 +526,8 @@ void record_wave_steps(rrg_ctx* c, int nsteps, bool prologue) {
         c->mg_cur = t;
     }
     for (int s = 0; s < nsteps; ++s) {
-        if (!solve_step_persistent(c, w, c->wave.iterations, false)) {
+        if (!solve_step_persistent(c, w, c->wave.iterations, false) &&
+            !solve_step_incremental(c, w, c->wave.iterations, false)) {
             wave_source(c, true);
             for (int k = 0; k < c->wave.iterations; ++k) wave_substep(c, w, nullptr);
             gradient(c);
@@ -1076,7 +1114,8 @@ RRG_API rrg_status rrg_solve_wave_and_field(rrg_ctx* ctx, int iterations) {
         RRG_REQUIRE(ctx->has_wave, RRG_ERR_STATE, "no wave parameters");
         RRG_REQUIRE(iterations >= 1, RRG_ERR_INVALID, "iterations must be >= 1");
         const WaveCoef w = wave_coef(ctx);
-        if (!solve_step_persistent(ctx, w, iterations, true)) {
+        if (!solve_step_persistent(ctx, w, iterations, true) &&
+            !solve_step_incremental(ctx, w, iterations, true)) {
             if (ctx->src_dirty || !ctx->src_valid) wave_source(ctx, false);
             for (int k = 0; k < iterations; ++k) wave_substep(ctx, w, nullptr);
             gradient(ctx);

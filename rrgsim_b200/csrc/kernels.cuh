@@ -147,13 +147,76 @@ __device__ __forceinline__ float4 wave_cell4(const float4 c, float lft, float rg
     return o;
 }
 
+// The wave source of one cell from its fixed-point deposit q (mass = q 2^-S): 4 pi G (rho -
+// rho_sub) with G = 1 and the reference's PI (co_info_structs.h:7), before any rounding to FP32.
+// Every FP32 source in the library is this value rounded.
+__device__ __forceinline__ double wave_source_value(unsigned long long q, double inv_scale,
+                                                    double inv_dx3, double rho_sub) {
+    const double mass = __dmul_rn(static_cast<double>(q), inv_scale);
+    const double rho = __dsub_rn(__dmul_rn(mass, inv_dx3), rho_sub);
+    return __dmul_rn(4.0 * 3.14159265358979, rho);
+}
+
+// Incremental form of one solve (the fused steps' FP32 / MIXED solves on periodic grids). With
+// the levels written phi = phi0 + d, phi0 the current level at the start of the solve, every
+// substep becomes
+//   d_new = K_MAIN L6(d) + K_ACTUAL d + K_OLD d_old + g,
+//   g     = K_F src + K_MAIN L6(phi0) + (K_ACTUAL + K_OLD - 1) phi0,
+// (L6: the sum of the six neighbours), starting from d = 0 and d_old = phi_prev - phi0. g is
+// evaluated once per solve in FP64 and rounded once; the increments are small next to phi, so
+// the FP32 rounding of 20 substeps lands on them instead of on phi, and phi0 + d is rounded once
+// at the end. kao = K_ACTUAL + K_OLD - 1. Arguments: src the FP64 source, l / r the x
+// neighbours, ym .. zp the y and z neighbours, c the cell, all of phi0.
+__device__ __forceinline__ float wave_inc_source(double src, float l, float r, float ym,
+                                                 float yp, float zm, float zp, float c,
+                                                 double kf, double km, double kao) {
+    double l6 = __dadd_rn(static_cast<double>(l), static_cast<double>(r));
+    l6 = __dadd_rn(l6, static_cast<double>(ym));
+    l6 = __dadd_rn(l6, static_cast<double>(yp));
+    l6 = __dadd_rn(l6, static_cast<double>(zm));
+    l6 = __dadd_rn(l6, static_cast<double>(zp));
+    return __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(kf, src), __dmul_rn(km, l6)),
+                                       __dmul_rn(kao, static_cast<double>(c))));
+}
+// four x-cells of a row (as wave_cell4); s: their FP64 sources
+__device__ __forceinline__ float4 wave_inc_source4(const double s[4], const float4 c, float lft,
+                                                   float rgt, const float4 ym, const float4 yp,
+                                                   const float4 zm, const float4 zp, double kf,
+                                                   double km, double kao) {
+    float4 o;
+    o.x = wave_inc_source(s[0], lft, c.y, ym.x, yp.x, zm.x, zp.x, c.x, kf, km, kao);
+    o.y = wave_inc_source(s[1], c.x, c.z, ym.y, yp.y, zm.y, zp.y, c.y, kf, km, kao);
+    o.z = wave_inc_source(s[2], c.y, c.w, ym.z, yp.z, zm.z, zp.z, c.z, kf, km, kao);
+    o.w = wave_inc_source(s[3], c.z, rgt, ym.w, yp.w, zm.w, zp.w, c.w, kf, km, kao);
+    return o;
+}
+__device__ __forceinline__ float4 f4_sub(const float4 a, const float4 b) {
+    return make_float4(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z),
+                       __fsub_rn(a.w, b.w));
+}
+__device__ __forceinline__ float4 f4_add(const float4 a, const float4 b) {
+    return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z),
+                       __fadd_rn(a.w, b.w));
+}
+
+// The incremental solve one launch per substep (the fused path where the persistent kernels do
+// not apply, and RRG_WAVE_PERSIST=0): prep writes g and d = 0, d_old = phi_prev - phi0; the
+// substeps run launch_wave_step on (d, d_old, g) with K_F = 1; finish writes phi0 + d_final and
+// phi0 + d_before into fin and prv (either may be phi0 itself). FP32 grids, periodic, uniform.
+void launch_wave_inc_prep(int nx, const unsigned long long* mg, int shift_s, double dx,
+                          double rho_sub, const float* phi0, const float* phi_prev,
+                          const WaveCoef& w, float* g, float* d, float* d_old, cudaStream_t s);
+void launch_wave_inc_finish(int nx, const float* phi0, const float* d_fin, const float* d_prv,
+                            float* fin, float* prv, cudaStream_t s);
+
 // One PM step's whole FP32 wave solve in one persistent cooperative kernel (wave_solve.cu):
 // source from the deposit mg (mg_zero cleared), `iterations` substeps over the levels phi0 /
 // phi1 (cur: which holds the current level; the result lands in phi[cur ^ (iterations & 1)],
 // the level before it in the other), then the gradient into acc4 (skipped when acc4 is null);
-// the source is also stored to src unless src is null.
-// Periodic box without an absorbing layer only; the same results as launch_wave_source +
-// launch_wave_step + launch_gradient. sync: wave_solve_sync_bytes(nx) of device memory, zeroed
+// the source is also stored to src unless src is null. The substeps run in the incremental form
+// (wave_inc_source): the same bits as launch_wave_inc_prep + launch_wave_step x iterations +
+// launch_wave_inc_finish + launch_gradient.
+// Periodic box without an absorbing layer only. sync: wave_solve_sync_bytes(nx) of device memory, zeroed
 // before the first use and kept between calls; its word at byte 65532 becomes non-zero when a
 // wait between blocks ran out (the step is then invalid and the memory must be zeroed again).
 // Returns false, launching nothing, where it does not apply (nx, residency,

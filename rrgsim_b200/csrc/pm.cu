@@ -142,17 +142,27 @@ __device__ __forceinline__ void cic_deposit_warp(bool active, double x, double y
     const bool head = lane == 0 || below != key;
     const bool tail = lane == 31 || above != key;
     const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const int first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // this run's first lane
     unsigned sum[8];
+    if (__popc(heads) <= 2) {
+        // one or two runs (warp-uniform; the common case in dense regions of sorted
+        // particles): one hardware reduction per run and corner instead of the scan
+        const unsigned second = heads & ~1u;  // the second run's head lane bit, or 0
+        const unsigned mask = second == 0u ? 0xffffffffu
+                              : ((lane < __ffs(second) - 1) ? second - 1u : ~(second - 1u));
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        unsigned v = q[c];
+        for (int c = 0; c < 8; ++c) sum[c] = __reduce_add_sync(mask, q[c]);
+    } else {
+        const int first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // the run's first lane
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const unsigned t = __shfl_up_sync(0xffffffffu, v, d);
-            if (lane - d >= first) v += t;
+        for (int c = 0; c < 8; ++c) {
+            unsigned v = q[c];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned t = __shfl_up_sync(0xffffffffu, v, d);
+                if (lane - d >= first) v += t;
+            }
+            sum[c] = v;  // at the run's last lane: the run's total
         }
-        sum[c] = v;  // at the run's last lane: the run's total
     }
     if (key >= 0 && tail) {
         // the run's cell and its corners (clamped as cic_axis clamps)
@@ -212,9 +222,50 @@ __global__ void wave_source_kernel(int64_t ncells, unsigned long long* __restric
     if (c >= ncells) return;
     const unsigned long long q = mgrid[c];
     if (zero_grid) mgrid[c] = 0ull;
-    const double mass = static_cast<double>(q) * inv_scale;
-    const double rho = (sizeof(R) == 8 ? mass / dx3 : mass * inv_dx3) - rho_sub;
-    src[c] = static_cast<R>(mult * (4.0 * kPi * 1.0 * rho));
+    if constexpr (sizeof(R) == 8) {
+        const double mass = static_cast<double>(q) * inv_scale;
+        const double rho = mass / dx3 - rho_sub;
+        src[c] = static_cast<R>(mult * (4.0 * kPi * 1.0 * rho));
+    } else {
+        src[c] = static_cast<R>(__dmul_rn(mult, wave_source_value(q, inv_scale, inv_dx3, rho_sub)));
+    }
+}
+
+// The incremental solve's preparation and finish (wave_inc_source): one thread per cell,
+// periodic neighbours.
+__global__ void wave_inc_prep_kernel(int nx, const unsigned long long* __restrict__ mg,
+                                     double inv_scale, double inv_dx3, double rho_sub,
+                                     const float* __restrict__ phi0,
+                                     const float* __restrict__ phi_prev, double kf, double km,
+                                     double kao, float* __restrict__ g, float* __restrict__ d,
+                                     float* __restrict__ d_old) {
+    const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int x = static_cast<int>(c % nx), y = static_cast<int>((c / nx) % nx),
+              z = static_cast<int>(c / (static_cast<int64_t>(nx) * nx));
+    const int64_t row = c - x, plane = static_cast<int64_t>(nx) * nx;
+    const int64_t cz = c - static_cast<int64_t>(z) * plane;
+    const float p = phi0[c];
+    const float l = phi0[row + (x == 0 ? nx - 1 : x - 1)];
+    const float r = phi0[row + (x == nx - 1 ? 0 : x + 1)];
+    const float ym = phi0[c + (y == 0 ? (nx - 1) * nx : -nx)];
+    const float yp = phi0[c + (y == nx - 1 ? -(nx - 1) * nx : nx)];
+    const float zm = phi0[cz + (z == 0 ? nx - 1 : z - 1) * plane];
+    const float zp = phi0[cz + (z == nx - 1 ? 0 : z + 1) * plane];
+    g[c] = wave_inc_source(wave_source_value(mg[c], inv_scale, inv_dx3, rho_sub), l, r, ym, yp, zm,
+                           zp, p, kf, km, kao);
+    d[c] = 0.f;
+    d_old[c] = __fsub_rn(phi_prev[c], p);
+}
+
+__global__ void wave_inc_finish_kernel(int64_t nc, const float* phi0, const float* d_fin,
+                                       const float* d_prv, float* fin, float* prv) {
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const float p = phi0[c], a = d_fin[c], b = d_prv[c];
+    fin[c] = __fadd_rn(p, a);
+    prv[c] = __fadd_rn(p, b);
 }
 
 // ----------------------------------------------------------------------------------------------
@@ -920,6 +971,23 @@ void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int s
         wave_source_kernel<float><<<div_up(nc, 256), 256, 0, s>>>(
             nc, mg, inv_scale, dx3, 1.0 / dx3, rho_mean, scale, static_cast<float*>(src),
             zero_grid);
+    RRG_LAUNCHED();
+}
+
+void launch_wave_inc_prep(int nx, const unsigned long long* mg, int shift_s, double dx,
+                          double rho_sub, const float* phi0, const float* phi_prev,
+                          const WaveCoef& w, float* g, float* d, float* d_old, cudaStream_t s) {
+    const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
+    wave_inc_prep_kernel<<<div_up(nc, 256), 256, 0, s>>>(
+        nx, mg, ldexp(1.0, -shift_s), 1.0 / (dx * dx * dx), rho_sub, phi0, phi_prev, w.K_F,
+        w.K_MAIN, w.K_ACTUAL + w.K_OLD - 1.0, g, d, d_old);
+    RRG_LAUNCHED();
+}
+
+void launch_wave_inc_finish(int nx, const float* phi0, const float* d_fin, const float* d_prv,
+                            float* fin, float* prv, cudaStream_t s) {
+    const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
+    wave_inc_finish_kernel<<<div_up(nc, 256), 256, 0, s>>>(nc, phi0, d_fin, d_prv, fin, prv);
     RRG_LAUNCHED();
 }
 

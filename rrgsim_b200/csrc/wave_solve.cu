@@ -108,7 +108,8 @@ struct SolveArgs {
     const unsigned long long* mg;   // this step's deposit
     unsigned long long* mg_zero;    // the other deposit grid: cleared
     double inv_scale, inv_dx3, rho_sub;
-    float km, ka, ko, kf, grad_coef;
+    float km, ka, ko, kf, grad_coef;  // kf = 1: the substeps run on increments (wave_inc_source)
+    double kf_d, km_d, kao_d;         // K_F, K_MAIN, K_ACTUAL + K_OLD - 1 for the increments' source
     float* src;                     // nullptr, or where the source is also stored
     float4* acc4;                   // nullptr: no gradient
     unsigned int* sync;             // sync_bytes_for(blocks), zeroed before the first launch
@@ -162,36 +163,21 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     const size_t col = (static_cast<size_t>(z0) * nx + y) * W + q;  // float4 index, plane z0
     constexpr size_t plane4 = static_cast<size_t>(nx) * W;
 
-    // ---- the column's levels and source --------------------------------------------------
+    // ---- the column's level 0 (phi0); the deposit's FP64 sources -------------------------
+    const float4* const c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
+    const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
+    const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
     float4 cur[ZC], old[ZC];
-    {
-        const float4* c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
-        const float4* p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
-        const ulonglong2* m2 = reinterpret_cast<const ulonglong2*>(a.mg);
-        ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
 #pragma unroll
-        for (int k = 0; k < ZC; ++k) {
-            const size_t o4 = col + k * plane4;
-            cur[k] = __ldcg(c4 + o4);
-            old[k] = __ldcg(p4 + o4);
-            const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
-            const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
-            const unsigned long long mq[4] = {m01.x, m01.y, m23.x, m23.y};
-            float sv[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const double mass = static_cast<double>(mq[e]) * a.inv_scale;
-                const double rho = mass * a.inv_dx3 - a.rho_sub;
-                sv[e] = static_cast<float>(1.0 * (4.0 * kPiW * 1.0 * rho));
-            }
-            const float4 s4 = make_float4(sv[0], sv[1], sv[2], sv[3]);
-            srcs[k * kThreads + tid] = s4;
-            if (a.src != nullptr) __stcg(reinterpret_cast<float4*>(a.src) + o4, s4);
-            const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
-            __stcg(z2 + 2 * o4, zz);
-            __stcg(z2 + 2 * o4 + 1, zz);
-        }
-    }
+    for (int k = 0; k < ZC; ++k) cur[k] = __ldcg(c4 + col + k * plane4);
+    auto source = [&](size_t o4, double sd[4]) {
+        const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
+        const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
+        sd[0] = wave_source_value(m01.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[1] = wave_source_value(m01.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[2] = wave_source_value(m23.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[3] = wave_source_value(m23.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+    };
     // lanes 0-3 of warp 0 watch one neighbour's counter each
     const unsigned int* watched = nullptr;
     if (tid < 4)
@@ -268,16 +254,63 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     for (int k = 0; k < ZC; ++k) store_faces(e0, k, cur[k]);
     publish(e0);
     if (!exchange(e0)) return;
+    // the increments' source g from phi0 and its halo (wave_inc_source); the plain source stored
+    // where asked, the other deposit cleared; then level 0 of the increments is zero everywhere
+    // and the one before it phi_prev - phi0
+    {
+        ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
+        float4 zm = zh[r * W + q];
+        const float4 ztop = zh[(RB + r) * W + q];
+#pragma unroll
+        for (int k = 0; k < ZC; ++k) {
+            const size_t o4 = col + k * plane4;
+            double sd[4];
+            source(o4, sd);
+            const float4 c = cur[k];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrc);
+            srcs[k * kThreads + tid] = wave_inc_source4(
+                sd, c, lft, rgt, tile[(k * (RB + 2) + r) * W + q],
+                tile[(k * (RB + 2) + r + 2) * W + q], zm, k + 1 < ZC ? cur[k + 1] : ztop,
+                a.kf_d, a.km_d, a.kao_d);
+            zm = c;
+            if (a.src != nullptr)
+                __stcg(reinterpret_cast<float4*>(a.src) + o4,
+                       make_float4(static_cast<float>(sd[0]), static_cast<float>(sd[1]),
+                                   static_cast<float>(sd[2]), static_cast<float>(sd[3])));
+            const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
+            __stcg(z2 + 2 * o4, zz);
+            __stcg(z2 + 2 * o4 + 1, zz);
+        }
+#pragma unroll
+        for (int k = 0; k < ZC; ++k) {
+            old[k] = f4_sub(__ldcg(p4 + col + k * plane4), cur[k]);
+            cur[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+        for (int i = tid; i < S::tileN; i += kThreads) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = tid; i < S::zhN; i += kThreads) zh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+    }
     for (int t = 0; t < a.iterations; ++t) {
+        const bool last = t + 1 == a.iterations;
         float4 zm = zh[r * W + q];
         const float4 ztop = zh[(RB + r) * W + q];
 #pragma unroll
         for (int k = 0; k < ZC; ++k) {
             const float4 out = cell(k, zm, k + 1 < ZC ? cur[k + 1] : ztop);
             zm = cur[k];
-            old[k] = cur[k];
-            cur[k] = out;
-            store_faces(e0 + t + 1, k, out);
+            if (last) {
+                // the solve's last substep: full levels, phi0 + d (phi0 read again: only this
+                // block writes its cells, after its last exchange)
+                const float4 p0 = __ldcg(c4 + col + k * plane4);
+                old[k] = f4_add(p0, cur[k]);
+                cur[k] = f4_add(p0, out);
+            } else {
+                old[k] = cur[k];
+                cur[k] = out;
+            }
+            store_faces(e0 + t + 1, k, cur[k]);
         }
         const unsigned int e = e0 + t + 1;
         publish(e);  // (its barrier also ends this substep's reads of the tile and halo)
@@ -429,43 +462,19 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
     const float4* const c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
     const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
     const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
-    // the source of four cells from the deposit (wave_source_kernel<float>'s expression)
-    auto source = [&](size_t o4) -> float4 {
+    // the FP64 sources of four cells from the deposit (wave_source_value)
+    auto source = [&](size_t o4, double sd[4]) {
         const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
         const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
-        const unsigned long long mq[4] = {m01.x, m01.y, m23.x, m23.y};
-        float sv[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const double mass = static_cast<double>(mq[e]) * a.inv_scale;
-            const double rho = mass * a.inv_dx3 - a.rho_sub;
-            sv[e] = static_cast<float>(1.0 * (4.0 * kPiW * 1.0 * rho));
-        }
-        return make_float4(sv[0], sv[1], sv[2], sv[3]);
+        sd[0] = wave_source_value(m01.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[1] = wave_source_value(m01.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[2] = wave_source_value(m23.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[3] = wave_source_value(m23.y, a.inv_scale, a.inv_dx3, a.rho_sub);
     };
 
-    // ---- level 0 and the level before it, the source, the halo: all from global memory ----
-#pragma unroll 1
-    for (int k = 0; k < KP; ++k) {
-        const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
-        const float4 s4 = source(o4);
-        srcs[k * T + tid] = s4;
-        if (k >= 1 && k <= ZC) {
-            if (a.src != nullptr) __stcg(reinterpret_cast<float4*>(a.src) + o4, s4);
-            ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
-            const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
-            __stcg(z2 + 2 * o4, zz);
-            __stcg(z2 + 2 * o4 + 1, zz);
-        }
-    }
-    float4 cur[KP], old[KP];
+    // ---- level 0 (phi0) and its halo from global memory into the tile ----------------------
 #pragma unroll
-    for (int k = 0; k < KP; ++k) {
-        const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
-        cur[k] = __ldcg(c4 + o4);
-        old[k] = __ldcg(p4 + o4);
-        T4(k, r + 2)[q] = cur[k];
-    }
+    for (int k = 0; k < KP; ++k) T4(k, r + 2)[q] = __ldcg(c4 + g4(z0 - 1 + k, y0 + r) + q);
     for (int i = tid; i < 4 * ZC * W; i += T) {  // rows y0-2, y0-1, y0+RB, y0+RB+1, own planes
         const int jj = i / (ZC * W), rem = i - jj * (ZC * W), kk = rem / W, qq = rem - kk * W;
         const int j = jj < 2 ? jj : RB + jj;
@@ -480,12 +489,61 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
         const int side = i / (RB * W), rem = i - side * (RB * W), rr = rem / W, qq = rem - rr * W;
         zh[i] = __ldcg(c4 + g4(side ? z0 + ZC + 1 : z0 - 2, y0 + rr) + qq);
     }
-    for (int i = tid; i < ringN; i += T) {  // the outer rows' previous level and source
+    for (int i = tid; i < ringN; i += T) {  // the outer rows' increment before level 0
         const int side = i / (ZC * W), rem = i - side * (ZC * W), kk = rem / W, qq = rem - kk * W;
         const size_t o4 = g4(z0 + kk, side ? y0 + RB : y0 - 1) + qq;
-        rold[i] = __ldcg(p4 + o4);
-        rsrc[i] = source(o4);
+        rold[i] = f4_sub(__ldcg(p4 + o4), __ldcg(c4 + o4));
     }
+    __syncthreads();
+
+    // ---- the increments' source g of the columns and of the outer rows (from phi0 and its
+    // halo); the plain source stored where asked, the other deposit cleared -------------------
+    {
+        const double kfd = a.kf_d, kmd = a.km_d, kao = a.kao_d;
+#pragma unroll 1
+        for (int k = 0; k < KP; ++k) {
+            const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
+            double sd[4];
+            source(o4, sd);
+            const float4 c = T4(k, r + 2)[q];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+            const float4 zm = k > 0 ? T4(k - 1, r + 2)[q] : zh[r * W + q];
+            const float4 zp = k + 1 < KP ? T4(k + 1, r + 2)[q] : zh[(RB + r) * W + q];
+            srcs[k * T + tid] = wave_inc_source4(sd, c, lft, rgt, T4(k, r + 1)[q],
+                                                 T4(k, r + 3)[q], zm, zp, kfd, kmd, kao);
+            if (k >= 1 && k <= ZC) {
+                if (a.src != nullptr)
+                    __stcg(reinterpret_cast<float4*>(a.src) + o4,
+                           make_float4(static_cast<float>(sd[0]), static_cast<float>(sd[1]),
+                                       static_cast<float>(sd[2]), static_cast<float>(sd[3])));
+                ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
+                const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
+                __stcg(z2 + 2 * o4, zz);
+                __stcg(z2 + 2 * o4 + 1, zz);
+            }
+        }
+        const int side = warp / ZC, kk = warp - side * ZC, k = kk + 1;
+        const int j = side ? RB + 2 : 1;
+        double sd[4];
+        source(g4(z0 + kk, side ? y0 + RB : y0 - 1) + q, sd);
+        const float4 c = T4(k, j)[q];
+        const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+        const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+        rsrc[(side * ZC + kk) * W + q] =
+            wave_inc_source4(sd, c, lft, rgt, T4(k, j - 1)[q], T4(k, j + 1)[q], T4(k - 1, j)[q],
+                             T4(k + 1, j)[q], kfd, kmd, kao);
+    }
+    // ---- level 0 of the increments is zero everywhere; the one before is phi_prev - phi0 ---
+    float4 cur[KP], old[KP];
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+        old[k] = f4_sub(__ldcg(p4 + g4(z0 - 1 + k, y0 + r) + q), T4(k, r + 2)[q]);
+        cur[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    for (int i = tid; i < tileN; i += T) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < zhN; i += T) zh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
 
     // lanes 0-7 of warp 0 watch one neighbour's counter each: y-, y+, z-, z+, then the
@@ -550,8 +608,11 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
         __syncthreads();
     };
     // substep B: the own cells (planes 1 .. ZC) one level on, from the tile and the columns'
-    // outer planes; faces stored under epoch e as they are computed
-    auto substep_b = [&](unsigned int e) {
+    // outer planes; faces stored under epoch e as they are computed. In the solve's last
+    // substep the own levels become full levels, phi0 + d (phi0 read again from global memory:
+    // only this block writes its cells, and only after its last exchange), so the last exchange
+    // brings the neighbours' full final level for the gradient.
+    auto substep_b = [&](unsigned int e, bool last) {
         float4 zm = cur[0];
 #pragma unroll
         for (int k = 1; k <= ZC; ++k) {
@@ -563,7 +624,16 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
             zm = c;
             old[k] = c;
             cur[k] = out;
-            store_faces(e, k, out);
+            if (!last) store_faces(e, k, out);
+        }
+        if (last) {
+#pragma unroll
+            for (int k = 1; k <= ZC; ++k) {
+                const float4 p0 = __ldcg(c4 + g4(z0 - 1 + k, y0 + r) + q);
+                old[k] = f4_add(p0, old[k]);
+                cur[k] = f4_add(p0, cur[k]);
+                store_faces(e, k, cur[k]);
+            }
         }
     };
     // publish epoch e (the barrier orders every thread's face stores and its reads of the tile
@@ -634,16 +704,15 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
     // ---- passes of two substeps, then an odd one -------------------------------------------
     unsigned int e = base;
     int par = 0;
-    for (int p = 0; p < a.iterations / 2; ++p) {
-        substep_a(par);
-        par ^= 1;
+    const int npairs = a.iterations / 2;
+    const int npasses = npairs + (a.iterations & 1);
+    for (int p = 0; p < npasses; ++p) {
+        if (p < npairs) {  // two substeps; an odd count ends with substep B alone
+            substep_a(par);
+            par ^= 1;
+        }
         ++e;
-        substep_b(e);
-        if (!exchange(e)) return;
-    }
-    if (a.iterations & 1) {
-        ++e;
-        substep_b(e);
+        substep_b(e, p + 1 == npasses);
         if (!exchange(e)) return;
     }
 
@@ -793,7 +862,10 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
     a.km = static_cast<float>(w.K_MAIN);
     a.ka = static_cast<float>(w.K_ACTUAL);
     a.ko = static_cast<float>(w.K_OLD);
-    a.kf = static_cast<float>(w.K_F);
+    a.kf = 1.0f;
+    a.kf_d = w.K_F;
+    a.km_d = w.K_MAIN;
+    a.kao_d = w.K_ACTUAL + w.K_OLD - 1.0;
     a.grad_coef = static_cast<float>(-1.0 / dx);
     a.src = src;
     a.acc4 = acc4;

@@ -419,20 +419,24 @@ def test_persistent_wave_solve_equals_one_launch_per_substep(monkeypatch, prec, 
         np.testing.assert_array_equal(g1[k], g0[k])
     for a, b in zip(w1, w0):
         np.testing.assert_array_equal(a, b)
-    # one kernel instead of source + substeps + gradient in each of the 9 steps
-    assert launches[0] + 9 * (iterations + 1) == launches[1]
+    # one kernel instead of the increments' preparation, the substeps, the finish and the
+    # gradient in each of the 9 steps
+    assert launches[0] + 9 * (iterations + 2) == launches[1]
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
 @pytest.mark.parametrize("nx", [64, 40, 128])
-def test_solve_wave_and_field_equals_separate_calls(prec, nx):
-    """The one-call solve (the persistent kernels on FP32 / MIXED 64^3 and 128^3; separate
-    launches on 40^3 and in FP64) leaves the same bits as solve_wave_equation +
-    calc_acceleration_field."""
+def test_solve_wave_and_field_against_separate_calls(monkeypatch, prec, nx):
+    """The one-call solve (the fused steps' solve). FP64: the same bits as
+    solve_wave_equation + calc_acceleration_field. FP32 / MIXED on periodic grids: the
+    incremental form (each solve advances increments over its first level, rounded into the
+    level once at the end), the same bits from the persistent kernels (64^3, 128^3) and from one
+    launch per substep (RRG_WAVE_PERSIST=0; 40^3 always), and against the FP64 oracle within
+    the bound of the separate calls, which advance the full levels in FP32."""
     pos, vel, m, s2, g, wp, phi0 = _wave_setup(nx, prec)
     wp.steady_check_step = 10 ** 6  # no steady checks inside the 7 substeps
-    out = []
-    for fused in (True, False):
+
+    def run(fused):
         with _ctx(prec, pos, vel, m, s2, g) as c:
             c.set_wave_params(wp)
             c.convert_particles_to_grid()
@@ -444,12 +448,31 @@ def test_solve_wave_and_field_equals_separate_calls(prec, nx):
                 it, _ = c.solve_wave_equation(7)
                 assert it == 7
                 c.calc_acceleration_field()
-            out.append((c.get_grid(), c.get_wave_state()))
-    (g1, w1), (g0, w0) = out
+            return c.get_grid(), c.get_wave_state()
+
+    (g1, w1), (g0, w0) = run(True), run(False)
+    if prec == "fp64":
+        for k in g1:
+            np.testing.assert_array_equal(g1[k], g0[k])
+        for a, b in zip(w1, w0):
+            np.testing.assert_array_equal(a, b)
+        return
+    monkeypatch.setenv("RRG_WAVE_PERSIST", "0")
+    g2, w2 = run(True)
     for k in g1:
-        np.testing.assert_array_equal(g1[k], g0[k])
-    for a, b in zip(w1, w0):
+        np.testing.assert_array_equal(g1[k], g2[k])
+    for a, b in zip(w1, w2):
         np.testing.assert_array_equal(a, b)
+    og = _orc_grid(g, wave_speed=wp.wave_speed, diss_base=wp.diss_base, bc_type=1,
+                   rho_mean=1.0 / (nx * g.dx) ** 3)
+    st = orc.WaveState(nx)
+    st.set_all(f32(phi0))
+    st.solve(og, g1["mass"], 7)
+    scale = np.max(np.abs(st.curr))
+    e_inc = np.max(np.abs(g1["grav"] - st.curr)) / scale
+    e_plain = np.max(np.abs(g0["grav"] - st.curr)) / scale
+    assert e_inc <= 2e-6 and e_inc <= 1.5 * e_plain + 1e-9
+    np.testing.assert_allclose(g1["grav"], g0["grav"], rtol=0, atol=4e-6 * scale)
 
 
 @pytest.mark.parametrize("nx", [64, 128])

@@ -124,6 +124,7 @@ struct rrg_ctx {
     int keep_layer = 0;
     Buf maxbits;
     Buf wsync;                       // the persistent solve's progress counters and error word
+    Buf winc;                        // the incremental solve's source and first increment (FP32)
     bool wave_solve_used = false;
 
     // reductions / transfers
@@ -264,60 +265,51 @@ void gradient(rrg_ctx* c) {
     launch_gradient(c->prec, c->grid.nx, c->grid.dx, c->phi[c->phi_cur].p, c->acc4.p, c->stream);
 }
 
-// The source, `iterations` substeps and the gradient as the persistent kernel, where it applies
-// (FP32 grids, periodic box without an absorbing layer, a grid whose blocks all fit on the GPU
-// at once). The results equal those of wave_source + wave_substep x iterations + gradient;
-// false: nothing launched, the caller launches those. store_src = false leaves the source grid
-// unwritten (marked stale): the fused steps never read it.
-bool solve_step_persistent(rrg_ctx* c, const WaveCoef& w, int iterations, bool store_src) {
-    if (c->prec == RRG_PREC_FP64 || c->bc_type != RRG_BC_PERIODIC || c->keep_layer) return false;
-    if (!launch_wave_solve(c->grid.nx, iterations, c->phi[0].as<float>(),
-                           c->phi[1].as<float>(), c->phi_cur,
-                           c->mg[c->mg_cur].as<unsigned long long>(),
-                           c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
-                           c->rho_mean, w, store_src ? c->src.as<float>() : nullptr,
-                           c->acc4.as<float4>(),
-                           c->wsync.as<unsigned int>(), c->wsync.bytes, c->stream))
-        return false;
-    if (iterations % 2 == 1) c->phi_cur = 1 - c->phi_cur;
-    c->src_dirty = false;
-    c->src_valid = store_src;
-    c->wave_solve_used = true;
-    return true;
+// the gradient of level phi[k] into acc4
+void gradient_after(rrg_ctx* c, int k) {
+    launch_gradient(c->prec, c->grid.nx, c->grid.dx, c->phi[k].p, c->acc4.p, c->stream);
 }
 
-// The same solve one launch per substep, where the persistent kernel does not apply (grid
-// size, RRG_WAVE_PERSIST=0, residency) on FP32 / MIXED periodic grids without an absorbing
-// layer: the incremental form (wave_inc_source), the same bits as the persistent kernel. The
-// increments and their source live in the field buffer (acc4: 4 floats per cell), which the
-// gradient rewrites at the end. False (nothing launched) on other grids.
+// One solve of the fused steps on FP32 / MIXED periodic grids without an absorbing layer, in
+// the incremental form (wave_inc_source): the preparation (the increments' source, the
+// increment before level 0, the plain source when store_src, the next deposit target cleared)
+// in one streaming launch, then the substeps and the gradient as the persistent kernel where it
+// applies (32, 64, 128 cells, all blocks resident at once, RRG_WAVE_PERSIST not 0), else one
+// launch per substep with the same bits. The source g and d_old live in winc; one launch per
+// substep keeps the other increment in the field buffer (acc4), which the gradient rewrites at
+// the end. False (nothing launched) on other grids and precisions.
 bool solve_step_incremental(rrg_ctx* c, const WaveCoef& w, int iterations, bool store_src) {
     if (c->prec == RRG_PREC_FP64 || c->bc_type != RRG_BC_PERIODIC || c->keep_layer) return false;
     const int nx = c->grid.nx;
     const size_t nc = static_cast<size_t>(nx) * nx * nx;
-    float* a4 = c->acc4.as<float>();
-    float* d[2] = {a4, a4 + nc};
-    float* g = a4 + 2 * nc;
+    float* g = c->winc.as<float>();
+    float* d_old = g + nc;
     float* phi0 = c->phi[c->phi_cur].as<float>();
-    float* prev = c->phi[1 - c->phi_cur].as<float>();
-    if (store_src) wave_source(c, false);
-    launch_wave_inc_prep(nx, c->mg[c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
-                         c->rho_mean, phi0, prev, w, g, d[0], d[1], c->stream);
-    // the persistent kernel clears the next deposit target too
-    RRG_CUDA(cudaMemsetAsync(c->mg[1 - c->mg_cur].p, 0, c->mg[1 - c->mg_cur].bytes, c->stream));
-    WaveCoef wi = w;
-    wi.K_F = 1.0;
-    int cur = 0;
-    for (int k = 0; k < iterations; ++k) {
-        launch_wave_step(c->prec, nx, d[cur], d[1 - cur], g, wi, nullptr, c->stream);
-        cur = 1 - cur;
+    launch_wave_inc_prep(nx, c->mg[c->mg_cur].as<unsigned long long>(),
+                         c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
+                         c->rho_mean, phi0, c->phi[1 - c->phi_cur].as<float>(), w, g, nullptr,
+                         d_old, store_src ? c->src.as<float>() : nullptr, c->stream);
+    if (launch_wave_solve(nx, iterations, c->phi[0].as<float>(), c->phi[1].as<float>(),
+                          c->phi_cur, g, d_old, c->grid.dx, w, c->acc4.as<float4>(),
+                          c->wsync.as<unsigned int>(), c->wsync.bytes, c->stream)) {
+        c->wave_solve_used = true;
+    } else {
+        float* d[2] = {c->acc4.as<float>(), d_old};
+        RRG_CUDA(cudaMemsetAsync(d[0], 0, nc * sizeof(float), c->stream));
+        WaveCoef wi = w;
+        wi.K_F = 1.0;
+        int cur = 0;
+        for (int k = 0; k < iterations; ++k) {
+            launch_wave_step(c->prec, nx, d[cur], d[1 - cur], g, wi, nullptr, c->stream);
+            cur = 1 - cur;
+        }
+        // final level into phi[phi_cur ^ (iterations & 1)], the one before into the other
+        const int fin = c->phi_cur ^ (iterations & 1);
+        launch_wave_inc_finish(nx, phi0, d[cur], d[1 - cur], c->phi[fin].as<float>(),
+                               c->phi[1 - fin].as<float>(), c->stream);
+        gradient_after(c, fin);
     }
-    // final level into phi[phi_cur ^ (iterations & 1)], the one before into the other
-    float* fin = c->phi[c->phi_cur ^ (iterations & 1)].as<float>();
-    float* prv = c->phi[1 - (c->phi_cur ^ (iterations & 1))].as<float>();
-    launch_wave_inc_finish(nx, phi0, d[cur], d[1 - cur], fin, prv, c->stream);
     if (iterations % 2 == 1) c->phi_cur = 1 - c->phi_cur;
-    gradient(c);
     c->src_dirty = false;
     c->src_valid = store_src;
     return true;
@@ -526,8 +518,7 @@ void record_wave_steps(rrg_ctx* c, int nsteps, bool prologue) {
         c->mg_cur = t;
     }
     for (int s = 0; s < nsteps; ++s) {
-        if (!solve_step_persistent(c, w, c->wave.iterations, false) &&
-            !solve_step_incremental(c, w, c->wave.iterations, false)) {
+        if (!solve_step_incremental(c, w, c->wave.iterations, false)) {
             wave_source(c, true);
             for (int k = 0; k < c->wave.iterations; ++k) wave_substep(c, w, nullptr);
             gradient(c);
@@ -914,6 +905,8 @@ RRG_API rrg_status rrg_init_grid(rrg_ctx* ctx, const rrg_grid_info* grid) {
         ctx->acc4.alloc(nc * v4b(ctx));
         ctx->maxbits.alloc(16);
         ctx->wsync.alloc(wave_solve_sync_bytes(grid->nx));
+        if (ctx->prec != RRG_PREC_FP64) ctx->winc.alloc(2 * nc * sizeof(float));
+        else ctx->winc.release();
         for (Buf* b : {&ctx->mg[0], &ctx->mg[1], &ctx->src, &ctx->phi[0], &ctx->phi[1],
                        &ctx->acc4, &ctx->maxbits, &ctx->wsync})
             RRG_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, ctx->stream));
@@ -1114,8 +1107,7 @@ RRG_API rrg_status rrg_solve_wave_and_field(rrg_ctx* ctx, int iterations) {
         RRG_REQUIRE(ctx->has_wave, RRG_ERR_STATE, "no wave parameters");
         RRG_REQUIRE(iterations >= 1, RRG_ERR_INVALID, "iterations must be >= 1");
         const WaveCoef w = wave_coef(ctx);
-        if (!solve_step_persistent(ctx, w, iterations, true) &&
-            !solve_step_incremental(ctx, w, iterations, true)) {
+        if (!solve_step_incremental(ctx, w, iterations, true)) {
             if (ctx->src_dirty || !ctx->src_valid) wave_source(ctx, false);
             for (int k = 0; k < iterations; ++k) wave_substep(ctx, w, nullptr);
             gradient(ctx);

@@ -199,23 +199,25 @@ __device__ __forceinline__ float4 f4_add(const float4 a, const float4 b) {
                        __fadd_rn(a.w, b.w));
 }
 
-// The incremental solve one launch per substep (the fused path where the persistent kernels do
-// not apply, and RRG_WAVE_PERSIST=0): prep writes g and d = 0, d_old = phi_prev - phi0; the
-// substeps run launch_wave_step on (d, d_old, g) with K_F = 1; finish writes phi0 + d_final and
+// The incremental solve's preparation, one streaming launch over the grid: g and
+// d_old = phi_prev - phi0 per cell, d = 0 (unless null), the plain FP32 source into src (unless
+// null), the next deposit target mg_zero cleared (unless null). The persistent kernels start from
+// g and d_old; one launch per substep (where they do not apply, and RRG_WAVE_PERSIST=0) runs
+// launch_wave_step on (d, d_old, g) with K_F = 1, and finish writes phi0 + d_final and
 // phi0 + d_before into fin and prv (either may be phi0 itself). FP32 grids, periodic, uniform.
-void launch_wave_inc_prep(int nx, const unsigned long long* mg, int shift_s, double dx,
-                          double rho_sub, const float* phi0, const float* phi_prev,
-                          const WaveCoef& w, float* g, float* d, float* d_old, cudaStream_t s);
+void launch_wave_inc_prep(int nx, const unsigned long long* mg, unsigned long long* mg_zero,
+                          int shift_s, double dx, double rho_sub, const float* phi0,
+                          const float* phi_prev, const WaveCoef& w, float* g, float* d,
+                          float* d_old, float* src, cudaStream_t s);
 void launch_wave_inc_finish(int nx, const float* phi0, const float* d_fin, const float* d_prv,
                             float* fin, float* prv, cudaStream_t s);
 
-// One PM step's whole FP32 wave solve in one persistent cooperative kernel (wave_solve.cu):
-// source from the deposit mg (mg_zero cleared), `iterations` substeps over the levels phi0 /
-// phi1 (cur: which holds the current level; the result lands in phi[cur ^ (iterations & 1)],
-// the level before it in the other), then the gradient into acc4 (skipped when acc4 is null);
-// the source is also stored to src unless src is null. The substeps run in the incremental form
-// (wave_inc_source): the same bits as launch_wave_inc_prep + launch_wave_step x iterations +
-// launch_wave_inc_finish + launch_gradient.
+// One PM step's FP32 wave solve after launch_wave_inc_prep, in one persistent cooperative
+// kernel (wave_solve.cu): `iterations` substeps on the increments from g and d_old (the prep's
+// outputs), the levels phi0 / phi1 (cur: which holds the current level, phi0 of the increments;
+// the result lands in phi[cur ^ (iterations & 1)], the level before it in the other), then the
+// gradient into acc4 (skipped when acc4 is null). The same bits as launch_wave_step x iterations
+// + launch_wave_inc_finish + launch_gradient after the same prep.
 // Periodic box without an absorbing layer only. sync: wave_solve_sync_bytes(nx) of device memory, zeroed
 // before the first use and kept between calls; its word at byte 65532 becomes non-zero when a
 // wait between blocks ran out (the step is then invalid and the memory must be zeroed again).
@@ -225,9 +227,8 @@ bool wave_solve_applicable(int nx);
 size_t wave_solve_sync_bytes(int nx);
 constexpr size_t kWaveSyncErrOffset = 65532;
 bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur,
-                       const unsigned long long* mg, unsigned long long* mg_zero, int shift_s,
-                       double dx, double rho_sub, const WaveCoef& w, float* src, float4* acc4,
-                       unsigned int* sync, size_t sync_bytes, cudaStream_t s);
+                       const float* g, const float* d_old, double dx, const WaveCoef& w,
+                       float4* acc4, unsigned int* sync, size_t sync_bytes, cudaStream_t s);
 // Trilinear gather of acc4 to particles (rm_mesh2p.cu:48-114).
 void launch_interp(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
                    const void* acc4, void* acc, cudaStream_t s);

@@ -234,11 +234,12 @@ __global__ void wave_source_kernel(int64_t ncells, unsigned long long* __restric
 // The incremental solve's preparation and finish (wave_inc_source): one thread per cell,
 // periodic neighbours.
 __global__ void wave_inc_prep_kernel(int nx, const unsigned long long* __restrict__ mg,
+                                     unsigned long long* __restrict__ mg_zero,
                                      double inv_scale, double inv_dx3, double rho_sub,
                                      const float* __restrict__ phi0,
                                      const float* __restrict__ phi_prev, double kf, double km,
                                      double kao, float* __restrict__ g, float* __restrict__ d,
-                                     float* __restrict__ d_old) {
+                                     float* __restrict__ d_old, float* __restrict__ src) {
     const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
     const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -253,10 +254,12 @@ __global__ void wave_inc_prep_kernel(int nx, const unsigned long long* __restric
     const float yp = phi0[c + (y == nx - 1 ? -(nx - 1) * nx : nx)];
     const float zm = phi0[cz + (z == 0 ? nx - 1 : z - 1) * plane];
     const float zp = phi0[cz + (z == nx - 1 ? 0 : z + 1) * plane];
-    g[c] = wave_inc_source(wave_source_value(mg[c], inv_scale, inv_dx3, rho_sub), l, r, ym, yp, zm,
-                           zp, p, kf, km, kao);
-    d[c] = 0.f;
+    const double sd = wave_source_value(mg[c], inv_scale, inv_dx3, rho_sub);
+    g[c] = wave_inc_source(sd, l, r, ym, yp, zm, zp, p, kf, km, kao);
+    if (d) d[c] = 0.f;
     d_old[c] = __fsub_rn(phi_prev[c], p);
+    if (src) src[c] = static_cast<float>(sd);
+    if (mg_zero) mg_zero[c] = 0ull;
 }
 
 __global__ void wave_inc_finish_kernel(int64_t nc, const float* phi0, const float* d_fin,
@@ -974,13 +977,14 @@ void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int s
     RRG_LAUNCHED();
 }
 
-void launch_wave_inc_prep(int nx, const unsigned long long* mg, int shift_s, double dx,
-                          double rho_sub, const float* phi0, const float* phi_prev,
-                          const WaveCoef& w, float* g, float* d, float* d_old, cudaStream_t s) {
+void launch_wave_inc_prep(int nx, const unsigned long long* mg, unsigned long long* mg_zero,
+                          int shift_s, double dx, double rho_sub, const float* phi0,
+                          const float* phi_prev, const WaveCoef& w, float* g, float* d,
+                          float* d_old, float* src, cudaStream_t s) {
     const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
     wave_inc_prep_kernel<<<div_up(nc, 256), 256, 0, s>>>(
-        nx, mg, ldexp(1.0, -shift_s), 1.0 / (dx * dx * dx), rho_sub, phi0, phi_prev, w.K_F,
-        w.K_MAIN, w.K_ACTUAL + w.K_OLD - 1.0, g, d, d_old);
+        nx, mg, mg_zero, ldexp(1.0, -shift_s), 1.0 / (dx * dx * dx), rho_sub, phi0, phi_prev,
+        w.K_F, w.K_MAIN, w.K_ACTUAL + w.K_OLD - 1.0, g, d, d_old, src);
     RRG_LAUNCHED();
 }
 

@@ -39,10 +39,12 @@ def _setup(prec):
     return c, m, og
 
 
-# Median relative error of the accelerations after one fused step from the same state, and of
-# the positions after three (FP32 compute; MIXED keeps double-float positions).
-ACC_TOL = {"fp32": 1e-4, "mixed": 1e-4}
-POS_TOL = {"fp32": 1e-6, "mixed": 1e-6}
+# Median relative error of the accelerations after one fused step from the same state (the
+# bar: 1e-5), and of the positions after three. FP32 advances full FP32 wave levels (measured
+# ~4e-6); MIXED advances increments over each solve's first level and keeps double-float
+# positions (measured 2.0e-7 after one step, 2.8e-7 after three).
+ACC_TOL = {"fp32": 1e-5, "mixed": 1e-6}
+POS_TOL = {"fp32": 1e-6, "mixed": 1e-8}
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])

@@ -124,7 +124,6 @@ struct rrg_ctx {
     int keep_layer = 0;
     Buf maxbits;
     Buf wsync;                       // the persistent solve's progress counters and error word
-    Buf winc;                        // the incremental solve's source and first increment (FP32)
     bool wave_solve_used = false;
 
     // reductions / transfers
@@ -270,65 +269,50 @@ void gradient_after(rrg_ctx* c, int k) {
     launch_gradient(c->prec, c->grid.nx, c->grid.dx, c->phi[k].p, c->acc4.p, c->stream);
 }
 
-// One solve of the fused steps (source, `iterations` substeps, gradient) on periodic grids
-// without an absorbing layer, as the persistent kernel where it applies (32, 64, 128 cells, all
-// blocks resident at once, RRG_WAVE_PERSIST not 0):
-// - FP32: full levels, the source from the deposit (the next deposit target cleared); the same
-//   bits as wave_source + wave_substep x iterations + gradient, which the caller launches when
-//   this returns false;
-// - MIXED: increments over the solve's first level (wave_inc_source), prepared by one streaming
-//   launch (the increments' source g and the increment before level 0 in winc, the plain source
-//   when store_src, the next deposit target cleared), then the persistent kernel, or where it
-//   does not apply one launch per substep with the same bits (the other increment in the field
-//   buffer acc4, which the gradient rewrites at the end). The FP32 roundings of the substeps
-//   land on the increments, and the level is rounded once at the end.
-// False (nothing launched) where neither applies: FP64, other boundaries, and FP32 grids the
-// persistent kernel does not take.
+// One solve of the fused steps (source, `iterations` substeps, gradient) on FP32 / MIXED
+// periodic grids without an absorbing layer, in the incremental form (wave_inc_source): each
+// solve advances increments over its first level, so the FP32 roundings of the substeps land on
+// the increments, and the level is rounded once at the end. It runs as the persistent kernel
+// where that applies (32, 64, 128 cells, all blocks resident at once, RRG_WAVE_PERSIST not 0),
+// else one launch per substep with the same bits: a preparation (the increments' source and
+// first increment, the plain source when store_src, the next deposit target cleared), the
+// substeps, the finish (the levels in full) and the gradient; the increments and their source
+// live in the field buffer (acc4: 4 floats per cell), which the gradient rewrites at the end.
+// False (nothing launched) on other grids and precisions: the caller launches the reference's
+// full-level form (wave_source + wave_substep x iterations + gradient).
 bool solve_step_fused(rrg_ctx* c, const WaveCoef& w, int iterations, bool store_src) {
     if (c->prec == RRG_PREC_FP64 || c->bc_type != RRG_BC_PERIODIC || c->keep_layer) return false;
     const int nx = c->grid.nx;
-    float* sync_phi0 = c->phi[0].as<float>();
-    float* sync_phi1 = c->phi[1].as<float>();
-    if (c->prec == RRG_PREC_FP32) {
-        if (!launch_wave_solve(nx, iterations, sync_phi0, sync_phi1, c->phi_cur,
-                               c->mg[c->mg_cur].as<unsigned long long>(),
-                               c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s,
-                               c->rho_mean, store_src ? c->src.as<float>() : nullptr, nullptr,
-                               nullptr, c->grid.dx, w, c->acc4.as<float4>(),
-                               c->wsync.as<unsigned int>(), c->wsync.bytes, c->stream))
-            return false;
+    if (launch_wave_solve(nx, iterations, c->phi[0].as<float>(), c->phi[1].as<float>(),
+                          c->phi_cur, c->mg[c->mg_cur].as<unsigned long long>(),
+                          c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s, c->grid.dx,
+                          c->rho_mean, w, store_src ? c->src.as<float>() : nullptr,
+                          c->acc4.as<float4>(), c->wsync.as<unsigned int>(), c->wsync.bytes,
+                          c->stream)) {
         c->wave_solve_used = true;
     } else {
         const size_t nc = static_cast<size_t>(nx) * nx * nx;
-        float* g = c->winc.as<float>();
-        float* d_old = g + nc;
+        float* a4 = c->acc4.as<float>();
+        float* d[2] = {a4, a4 + nc};
+        float* g = a4 + 2 * nc;
         float* phi0 = c->phi[c->phi_cur].as<float>();
         launch_wave_inc_prep(nx, c->mg[c->mg_cur].as<unsigned long long>(),
                              c->mg[1 - c->mg_cur].as<unsigned long long>(), c->shift_s,
                              c->grid.dx, c->rho_mean, phi0, c->phi[1 - c->phi_cur].as<float>(),
-                             w, g, nullptr, d_old, store_src ? c->src.as<float>() : nullptr,
+                             w, g, d[0], d[1], store_src ? c->src.as<float>() : nullptr,
                              c->stream);
-        if (launch_wave_solve(nx, iterations, sync_phi0, sync_phi1, c->phi_cur, nullptr, nullptr,
-                              c->shift_s, c->rho_mean, nullptr, g, d_old, c->grid.dx, w,
-                              c->acc4.as<float4>(), c->wsync.as<unsigned int>(), c->wsync.bytes,
-                              c->stream)) {
-            c->wave_solve_used = true;
-        } else {
-            float* d[2] = {c->acc4.as<float>(), d_old};
-            RRG_CUDA(cudaMemsetAsync(d[0], 0, nc * sizeof(float), c->stream));
-            WaveCoef wi = w;
-            wi.K_F = 1.0;
-            int cur = 0;
-            for (int k = 0; k < iterations; ++k) {
-                launch_wave_step(c->prec, nx, d[cur], d[1 - cur], g, wi, nullptr, c->stream);
-                cur = 1 - cur;
-            }
-            // final level into phi[phi_cur ^ (iterations & 1)], the one before into the other
-            const int fin = c->phi_cur ^ (iterations & 1);
-            launch_wave_inc_finish(nx, phi0, d[cur], d[1 - cur], c->phi[fin].as<float>(),
-                                   c->phi[1 - fin].as<float>(), c->stream);
-            gradient_after(c, fin);
+        WaveCoef wi = w;
+        wi.K_F = 1.0;
+        int cur = 0;
+        for (int k = 0; k < iterations; ++k) {
+            launch_wave_step(c->prec, nx, d[cur], d[1 - cur], g, wi, nullptr, c->stream);
+            cur = 1 - cur;
         }
+        // final level into phi[phi_cur ^ (iterations & 1)], the one before into the other
+        const int fin = c->phi_cur ^ (iterations & 1);
+        launch_wave_inc_finish(nx, phi0, d[cur], d[1 - cur], c->phi[fin].as<float>(),
+                               c->phi[1 - fin].as<float>(), c->stream);
+        gradient_after(c, fin);
     }
     if (iterations % 2 == 1) c->phi_cur = 1 - c->phi_cur;
     c->src_dirty = false;
@@ -926,8 +910,6 @@ RRG_API rrg_status rrg_init_grid(rrg_ctx* ctx, const rrg_grid_info* grid) {
         ctx->acc4.alloc(nc * v4b(ctx));
         ctx->maxbits.alloc(16);
         ctx->wsync.alloc(wave_solve_sync_bytes(grid->nx));
-        if (ctx->prec == RRG_PREC_MIXED) ctx->winc.alloc(2 * nc * sizeof(float));
-        else ctx->winc.release();
         for (Buf* b : {&ctx->mg[0], &ctx->mg[1], &ctx->src, &ctx->phi[0], &ctx->phi[1],
                        &ctx->acc4, &ctx->maxbits, &ctx->wsync})
             RRG_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, ctx->stream));

@@ -201,9 +201,9 @@ __device__ __forceinline__ float4 f4_add(const float4 a, const float4 b) {
 
 // The incremental solve's preparation, one streaming launch over the grid: g and
 // d_old = phi_prev - phi0 per cell, d = 0 (unless null), the plain FP32 source into src (unless
-// null), the next deposit target mg_zero cleared (unless null). The persistent kernels start from
-// g and d_old; one launch per substep (where they do not apply, and RRG_WAVE_PERSIST=0) runs
-// launch_wave_step on (d, d_old, g) with K_F = 1, and finish writes phi0 + d_final and
+// null), the next deposit target mg_zero cleared (unless null). One launch per substep (where
+// the persistent kernels do not apply, and RRG_WAVE_PERSIST=0) then runs launch_wave_step on
+// (d, d_old, g) with K_F = 1, and finish writes phi0 + d_final and
 // phi0 + d_before into fin and prv (either may be phi0 itself). FP32 grids, periodic, uniform.
 void launch_wave_inc_prep(int nx, const unsigned long long* mg, unsigned long long* mg_zero,
                           int shift_s, double dx, double rho_sub, const float* phi0,
@@ -212,16 +212,13 @@ void launch_wave_inc_prep(int nx, const unsigned long long* mg, unsigned long lo
 void launch_wave_inc_finish(int nx, const float* phi0, const float* d_fin, const float* d_prv,
                             float* fin, float* prv, cudaStream_t s);
 
-// One PM step's FP32 wave solve in one persistent cooperative kernel (wave_solve.cu), over the
-// levels phi0 / phi1 (cur: which holds the current level; the result lands in
-// phi[cur ^ (iterations & 1)], the level before it in the other), then the gradient into acc4
-// (skipped when acc4 is null). Two forms, each with the bits of its one-launch-per-substep
-// counterpart:
-// - full levels (g null, FP32): the source from the deposit mg (mg_zero cleared, the source also
-//   stored to src unless null), as launch_wave_source + launch_wave_step x iterations +
-//   launch_gradient;
-// - increments (g non-null, MIXED): after launch_wave_inc_prep, from its g and d_old, as
-//   launch_wave_step x iterations on the increments + launch_wave_inc_finish + launch_gradient.
+// One PM step's whole FP32 wave solve in one persistent cooperative kernel (wave_solve.cu):
+// source from the deposit mg (mg_zero cleared), `iterations` substeps over the levels phi0 /
+// phi1 (cur: which holds the current level; the result lands in phi[cur ^ (iterations & 1)],
+// the level before it in the other), then the gradient into acc4 (skipped when acc4 is null);
+// the source is also stored to src unless src is null. The substeps run in the incremental form
+// (wave_inc_source): the same bits as launch_wave_inc_prep + launch_wave_step x iterations +
+// launch_wave_inc_finish + launch_gradient.
 // Periodic box without an absorbing layer only. sync: wave_solve_sync_bytes(nx) of device memory, zeroed
 // before the first use and kept between calls; its word at byte 65532 becomes non-zero when a
 // wait between blocks ran out (the step is then invalid and the memory must be zeroed again).
@@ -232,9 +229,8 @@ size_t wave_solve_sync_bytes(int nx);
 constexpr size_t kWaveSyncErrOffset = 65532;
 bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur,
                        const unsigned long long* mg, unsigned long long* mg_zero, int shift_s,
-                       double rho_sub, float* src, const float* g, const float* d_old,
-                       double dx, const WaveCoef& w, float4* acc4, unsigned int* sync,
-                       size_t sync_bytes, cudaStream_t s);
+                       double dx, double rho_sub, const WaveCoef& w, float* src, float4* acc4,
+                       unsigned int* sync, size_t sync_bytes, cudaStream_t s);
 // Trilinear gather of acc4 to particles (rm_mesh2p.cu:48-114).
 void launch_interp(int prec, int64_t n, const void* posm, const void* poslo, const GridDev& g,
                    const void* acc4, void* acc, cudaStream_t s);

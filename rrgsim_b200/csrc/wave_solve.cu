@@ -54,6 +54,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kZC = 8;                          // planes per block
+constexpr double kPiW = 3.14159265358979;       // the reference's PI (co_info_structs.h:7)
 constexpr long long kWaitCycles = 1ll << 28;    // ~0.14 s at 1.9 GHz per wait at most
 constexpr int kCounterStride = 32;              // a block's epoch counter: 128 bytes apart
 constexpr int kErrWord = 16383;                 // in the first 64 KB: counters, error word
@@ -104,40 +105,17 @@ struct SolveArgs {
     float* phi1;
     int cur;                        // phi_cur at entry: 0 -> phi0 is the current level
     int iterations;
-    // full levels (FP32): the source from the deposit
     const unsigned long long* mg;   // this step's deposit
     unsigned long long* mg_zero;    // the other deposit grid: cleared
     double inv_scale, inv_dx3, rho_sub;
+    float km, ka, ko, kf, grad_coef;  // kf = 1: the substeps run on increments (wave_inc_source)
+    double kf_d, km_d, kao_d;         // K_F, K_MAIN, K_ACTUAL + K_OLD - 1 for the increments' source
     float* src;                     // nullptr, or where the source is also stored
-    // increments (MIXED): from launch_wave_inc_prep
-    const float* g;                 // the increments' source
-    const float* d_old;             // the increment before level 0: phi_prev - phi_cur
-    float km, ka, ko, kf, grad_coef;  // kf = K_F for full levels, 1 for increments
     float4* acc4;                   // nullptr: no gradient
-    unsigned int* sync;             // sync memory, zeroed before the first launch
+    unsigned int* sync;             // sync_bytes_for(blocks), zeroed before the first launch
 };
 
-// the FP32 source of four cells from the deposit (wave_source_value, rounded)
-__device__ __forceinline__ float4 source4(const SolveArgs& a, size_t o4) {
-    const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
-    const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
-    const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
-    return make_float4(static_cast<float>(wave_source_value(m01.x, a.inv_scale, a.inv_dx3, a.rho_sub)),
-                       static_cast<float>(wave_source_value(m01.y, a.inv_scale, a.inv_dx3, a.rho_sub)),
-                       static_cast<float>(wave_source_value(m23.x, a.inv_scale, a.inv_dx3, a.rho_sub)),
-                       static_cast<float>(wave_source_value(m23.y, a.inv_scale, a.inv_dx3, a.rho_sub)));
-}
-
-// the source of cells o4 stored where asked, and their next deposit target cleared
-__device__ __forceinline__ void own_source_chores(const SolveArgs& a, size_t o4, const float4 s4) {
-    if (a.src != nullptr) __stcg(reinterpret_cast<float4*>(a.src) + o4, s4);
-    ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
-    const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
-    __stcg(z2 + 2 * o4, zz);
-    __stcg(z2 + 2 * o4 + 1, zz);
-}
-
-template <int W, bool INC>
+template <int W>
 __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs a) {
     using S = Shape<W>;
     constexpr int nx = S::nx, RB = S::RB, ZC = kZC;
@@ -185,33 +163,21 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     const size_t col = (static_cast<size_t>(z0) * nx + y) * W + q;  // float4 index, plane z0
     constexpr size_t plane4 = static_cast<size_t>(nx) * W;
 
-    // ---- the column: full levels and their source (FP32), or increments (MIXED), whose level 0
-    // is zero (its halo too) and whose level before and source come from the preparation ------
+    // ---- the column's level 0 (phi0); the deposit's FP64 sources -------------------------
     const float4* const c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
+    const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
+    const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
     float4 cur[ZC], old[ZC];
-    if constexpr (INC) {
 #pragma unroll
-        for (int k = 0; k < ZC; ++k) {
-            const size_t o4 = col + k * plane4;
-            old[k] = __ldcg(reinterpret_cast<const float4*>(a.d_old) + o4);
-            srcs[k * kThreads + tid] = __ldcg(reinterpret_cast<const float4*>(a.g) + o4);
-            cur[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        for (int i = tid; i < S::tileN; i += kThreads) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int i = tid; i < S::zhN; i += kThreads) zh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        __syncthreads();
-    } else {
-        const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
-#pragma unroll
-        for (int k = 0; k < ZC; ++k) {
-            const size_t o4 = col + k * plane4;
-            cur[k] = __ldcg(c4 + o4);
-            old[k] = __ldcg(p4 + o4);
-            const float4 s4 = source4(a, o4);
-            srcs[k * kThreads + tid] = s4;
-            own_source_chores(a, o4, s4);
-        }
-    }
+    for (int k = 0; k < ZC; ++k) cur[k] = __ldcg(c4 + col + k * plane4);
+    auto source = [&](size_t o4, double sd[4]) {
+        const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
+        const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
+        sd[0] = wave_source_value(m01.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[1] = wave_source_value(m01.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[2] = wave_source_value(m23.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[3] = wave_source_value(m23.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+    };
     // lanes 0-3 of warp 0 watch one neighbour's counter each
     const unsigned int* watched = nullptr;
     if (tid < 4)
@@ -283,14 +249,48 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     };
 
     // ---- substeps --------------------------------------------------------------------------
-    // level t is published as epoch e0 + t; level 0 of the increments needs no exchange (it is
-    // zero), level 0 of full levels does
-    const unsigned int e0 = INC ? base : base + 1;
-    if constexpr (!INC) {
+    const unsigned int e0 = base + 1;   // epoch of level 0; level t has e0 + t
 #pragma unroll
-        for (int k = 0; k < ZC; ++k) store_faces(e0, k, cur[k]);
-        publish(e0);
-        if (!exchange(e0)) return;
+    for (int k = 0; k < ZC; ++k) store_faces(e0, k, cur[k]);
+    publish(e0);
+    if (!exchange(e0)) return;
+    // the increments' source g from phi0 and its halo (wave_inc_source); the plain source stored
+    // where asked, the other deposit cleared; then level 0 of the increments is zero everywhere
+    // and the one before it phi_prev - phi0
+    {
+        ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
+        float4 zm = zh[r * W + q];
+        const float4 ztop = zh[(RB + r) * W + q];
+#pragma unroll
+        for (int k = 0; k < ZC; ++k) {
+            const size_t o4 = col + k * plane4;
+            double sd[4];
+            source(o4, sd);
+            const float4 c = cur[k];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrc);
+            srcs[k * kThreads + tid] = wave_inc_source4(
+                sd, c, lft, rgt, tile[(k * (RB + 2) + r) * W + q],
+                tile[(k * (RB + 2) + r + 2) * W + q], zm, k + 1 < ZC ? cur[k + 1] : ztop,
+                a.kf_d, a.km_d, a.kao_d);
+            zm = c;
+            if (a.src != nullptr)
+                __stcg(reinterpret_cast<float4*>(a.src) + o4,
+                       make_float4(static_cast<float>(sd[0]), static_cast<float>(sd[1]),
+                                   static_cast<float>(sd[2]), static_cast<float>(sd[3])));
+            const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
+            __stcg(z2 + 2 * o4, zz);
+            __stcg(z2 + 2 * o4 + 1, zz);
+        }
+#pragma unroll
+        for (int k = 0; k < ZC; ++k) {
+            old[k] = f4_sub(__ldcg(p4 + col + k * plane4), cur[k]);
+            cur[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+        for (int i = tid; i < S::tileN; i += kThreads) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = tid; i < S::zhN; i += kThreads) zh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
     }
     for (int t = 0; t < a.iterations; ++t) {
         const bool last = t + 1 == a.iterations;
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
         for (int k = 0; k < ZC; ++k) {
             const float4 out = cell(k, zm, k + 1 < ZC ? cur[k + 1] : ztop);
             zm = cur[k];
-            if (INC && last) {
+            if (last) {
                 // the solve's last substep: full levels, phi0 + d (phi0 read again: only this
                 // block writes its cells, after its last exchange)
                 const float4 p0 = __ldcg(c4 + col + k * plane4);
@@ -421,7 +421,6 @@ size_t sync_bytes_tb(int64_t nblocks) {
     return kFaceOffset + static_cast<size_t>(nblocks) * 2 * tb::FB * sizeof(float4);
 }
 
-template <bool INC>
 __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs a) {
     using namespace tb;
     extern __shared__ __align__(16) float4 sm[];
@@ -461,66 +460,90 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
     };
     const float km = a.km, ka = a.ka, ko = a.ko, kf = a.kf;
     const float4* const c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
-    const float4* const gp = reinterpret_cast<const float4*>(a.g);
-    const float4* const dp = reinterpret_cast<const float4*>(a.d_old);
+    const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
+    const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
+    // the FP64 sources of four cells from the deposit (wave_source_value)
+    auto source = [&](size_t o4, double sd[4]) {
+        const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
+        const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
+        sd[0] = wave_source_value(m01.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[1] = wave_source_value(m01.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[2] = wave_source_value(m23.x, a.inv_scale, a.inv_dx3, a.rho_sub);
+        sd[3] = wave_source_value(m23.y, a.inv_scale, a.inv_dx3, a.rho_sub);
+    };
 
-    float4 cur[KP], old[KP];
-    if constexpr (INC) {
-        // ---- the increments: level 0 is zero (its halo too); the one before and the source of
-        // the ten-plane columns and of the outer rows come from the preparation
+    // ---- level 0 (phi0) and its halo from global memory into the tile ----------------------
 #pragma unroll
-        for (int k = 0; k < KP; ++k) {
-            const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
-            old[k] = __ldcg(dp + o4);
-            srcs[k * T + tid] = __ldcg(gp + o4);
-            cur[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        for (int i = tid; i < ringN; i += T) {
-            const int side = i / (ZC * W), rem = i - side * (ZC * W), kk = rem / W, qq = rem - kk * W;
-            const size_t o4 = g4(z0 + kk, side ? y0 + RB : y0 - 1) + qq;
-            rold[i] = __ldcg(dp + o4);
-            rsrc[i] = __ldcg(gp + o4);
-        }
-        for (int i = tid; i < tileN; i += T) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int i = tid; i < zhN; i += T) zh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    } else {
-        // ---- full levels 0 and -1, the source, the halo: all from global memory
-        const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
+    for (int k = 0; k < KP; ++k) T4(k, r + 2)[q] = __ldcg(c4 + g4(z0 - 1 + k, y0 + r) + q);
+    for (int i = tid; i < 4 * ZC * W; i += T) {  // rows y0-2, y0-1, y0+RB, y0+RB+1, own planes
+        const int jj = i / (ZC * W), rem = i - jj * (ZC * W), kk = rem / W, qq = rem - kk * W;
+        const int j = jj < 2 ? jj : RB + jj;
+        T4(kk + 1, j)[qq] = __ldcg(c4 + g4(z0 + kk, y0 - 2 + j) + qq);
+    }
+    for (int i = tid; i < 4 * W; i += T) {  // the four edge rows
+        const int cc = i / W, qq = i - cc * W;
+        const int j = (cc & 1) ? RB + 2 : 1, k = (cc & 2) ? KP - 1 : 0;
+        T4(k, j)[qq] = __ldcg(c4 + g4(z0 - 1 + k, y0 - 2 + j) + qq);
+    }
+    for (int i = tid; i < zhN; i += T) {  // planes z0 - 2 and z0 + ZC + 1 of the own rows
+        const int side = i / (RB * W), rem = i - side * (RB * W), rr = rem / W, qq = rem - rr * W;
+        zh[i] = __ldcg(c4 + g4(side ? z0 + ZC + 1 : z0 - 2, y0 + rr) + qq);
+    }
+    for (int i = tid; i < ringN; i += T) {  // the outer rows' increment before level 0
+        const int side = i / (ZC * W), rem = i - side * (ZC * W), kk = rem / W, qq = rem - kk * W;
+        const size_t o4 = g4(z0 + kk, side ? y0 + RB : y0 - 1) + qq;
+        rold[i] = f4_sub(__ldcg(p4 + o4), __ldcg(c4 + o4));
+    }
+    __syncthreads();
+
+    // ---- the increments' source g of the columns and of the outer rows (from phi0 and its
+    // halo); the plain source stored where asked, the other deposit cleared -------------------
+    {
+        const double kfd = a.kf_d, kmd = a.km_d, kao = a.kao_d;
 #pragma unroll 1
         for (int k = 0; k < KP; ++k) {
             const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
-            const float4 s4 = source4(a, o4);
-            srcs[k * T + tid] = s4;
-            if (k >= 1 && k <= ZC) own_source_chores(a, o4, s4);
+            double sd[4];
+            source(o4, sd);
+            const float4 c = T4(k, r + 2)[q];
+            const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+            const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+            const float4 zm = k > 0 ? T4(k - 1, r + 2)[q] : zh[r * W + q];
+            const float4 zp = k + 1 < KP ? T4(k + 1, r + 2)[q] : zh[(RB + r) * W + q];
+            srcs[k * T + tid] = wave_inc_source4(sd, c, lft, rgt, T4(k, r + 1)[q],
+                                                 T4(k, r + 3)[q], zm, zp, kfd, kmd, kao);
+            if (k >= 1 && k <= ZC) {
+                if (a.src != nullptr)
+                    __stcg(reinterpret_cast<float4*>(a.src) + o4,
+                           make_float4(static_cast<float>(sd[0]), static_cast<float>(sd[1]),
+                                       static_cast<float>(sd[2]), static_cast<float>(sd[3])));
+                ulonglong2* z2 = reinterpret_cast<ulonglong2*>(a.mg_zero);
+                const ulonglong2 zz = make_ulonglong2(0ull, 0ull);
+                __stcg(z2 + 2 * o4, zz);
+                __stcg(z2 + 2 * o4 + 1, zz);
+            }
         }
-#pragma unroll
-        for (int k = 0; k < KP; ++k) {
-            const size_t o4 = g4(z0 - 1 + k, y0 + r) + q;
-            cur[k] = __ldcg(c4 + o4);
-            old[k] = __ldcg(p4 + o4);
-            T4(k, r + 2)[q] = cur[k];
-        }
-        for (int i = tid; i < 4 * ZC * W; i += T) {  // rows y0-2, y0-1, y0+RB, y0+RB+1
-            const int jj = i / (ZC * W), rem = i - jj * (ZC * W), kk = rem / W, qq = rem - kk * W;
-            const int j = jj < 2 ? jj : RB + jj;
-            T4(kk + 1, j)[qq] = __ldcg(c4 + g4(z0 + kk, y0 - 2 + j) + qq);
-        }
-        for (int i = tid; i < 4 * W; i += T) {  // the four edge rows
-            const int cc = i / W, qq = i - cc * W;
-            const int j = (cc & 1) ? RB + 2 : 1, k = (cc & 2) ? KP - 1 : 0;
-            T4(k, j)[qq] = __ldcg(c4 + g4(z0 - 1 + k, y0 - 2 + j) + qq);
-        }
-        for (int i = tid; i < zhN; i += T) {  // planes z0 - 2 and z0 + ZC + 1 of the own rows
-            const int side = i / (RB * W), rem = i - side * (RB * W), rr = rem / W, qq = rem - rr * W;
-            zh[i] = __ldcg(c4 + g4(side ? z0 + ZC + 1 : z0 - 2, y0 + rr) + qq);
-        }
-        for (int i = tid; i < ringN; i += T) {  // the outer rows' level before and source
-            const int side = i / (ZC * W), rem = i - side * (ZC * W), kk = rem / W, qq = rem - kk * W;
-            const size_t o4 = g4(z0 + kk, side ? y0 + RB : y0 - 1) + qq;
-            rold[i] = __ldcg(p4 + o4);
-            rsrc[i] = source4(a, o4);
-        }
+        const int side = warp / ZC, kk = warp - side * ZC, k = kk + 1;
+        const int j = side ? RB + 2 : 1;
+        double sd[4];
+        source(g4(z0 + kk, side ? y0 + RB : y0 - 1) + q, sd);
+        const float4 c = T4(k, j)[q];
+        const float lft = __shfl_sync(0xffffffffu, c.w, lsrc);
+        const float rgt = __shfl_sync(0xffffffffu, c.x, rsrcl);
+        rsrc[(side * ZC + kk) * W + q] =
+            wave_inc_source4(sd, c, lft, rgt, T4(k, j - 1)[q], T4(k, j + 1)[q], T4(k - 1, j)[q],
+                             T4(k + 1, j)[q], kfd, kmd, kao);
     }
+    // ---- level 0 of the increments is zero everywhere; the one before is phi_prev - phi0 ---
+    float4 cur[KP], old[KP];
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+        old[k] = f4_sub(__ldcg(p4 + g4(z0 - 1 + k, y0 + r) + q), T4(k, r + 2)[q]);
+        cur[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    for (int i = tid; i < tileN; i += T) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < zhN; i += T) zh[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
 
     // lanes 0-7 of warp 0 watch one neighbour's counter each: y-, y+, z-, z+, then the
@@ -606,11 +629,9 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
         if (last) {
 #pragma unroll
             for (int k = 1; k <= ZC; ++k) {
-                if constexpr (INC) {
-                    const float4 p0 = __ldcg(c4 + g4(z0 - 1 + k, y0 + r) + q);
-                    old[k] = f4_add(p0, old[k]);
-                    cur[k] = f4_add(p0, cur[k]);
-                }
+                const float4 p0 = __ldcg(c4 + g4(z0 - 1 + k, y0 + r) + q);
+                old[k] = f4_add(p0, old[k]);
+                cur[k] = f4_add(p0, cur[k]);
                 store_faces(e, k, cur[k]);
             }
         }
@@ -758,24 +779,18 @@ bool use_tb() {
     return on;
 }
 
-template <int W, bool INC>
+template <int W>
 void set_smem_attr() {
-    RRG_CUDA(cudaFuncSetAttribute(wave_solve_kernel<W, INC>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RRG_CUDA(cudaFuncSetAttribute(wave_solve_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(Shape<W>::smem)));
 }
 
 template <int W>
 int blocks_per_sm() {
     int per_sm = 0;
-    RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_solve_kernel<W, false>,
+    RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_solve_kernel<W>,
                                                            kThreads, Shape<W>::smem));
     return per_sm;
-}
-
-template <typename K>
-void launch_coop(cudaLaunchConfig_t& cfg, K kernel, const SolveArgs& a) {
-    RRG_CUDA(cudaLaunchKernelEx(&cfg, kernel, a));
 }
 
 int64_t block_count(int nx) {
@@ -799,11 +814,9 @@ size_t wave_solve_sync_bytes(int nx) {
 
 bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur,
                        const unsigned long long* mg, unsigned long long* mg_zero, int shift_s,
-                       double rho_sub, float* src, const float* g, const float* d_old,
-                       double dx, const WaveCoef& w, float4* acc4, unsigned int* sync,
-                       size_t sync_bytes, cudaStream_t s) {
+                       double dx, double rho_sub, const WaveCoef& w, float* src, float4* acc4,
+                       unsigned int* sync, size_t sync_bytes, cudaStream_t s) {
     if (!wave_solve_applicable(nx) || iterations < 1) return false;
-    const bool inc = g != nullptr;
     const bool tbk = nx == 128 && use_tb();
     const int W = nx / 4, RB = (tbk ? tb::T : kThreads) / W;
     const dim3 grid(nx / RB, nx / kZC);
@@ -811,8 +824,6 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
     RRG_REQUIRE(nblocks * kCounterStride < kErrWord &&
                     sync_bytes >= (tbk ? sync_bytes_tb(nblocks) : sync_bytes_for(nblocks)),
                 RRG_ERR_INVALID, "wave solve: sync memory too small for the grid");
-    RRG_REQUIRE(inc ? d_old != nullptr : (mg != nullptr && mg_zero != nullptr), RRG_ERR_INVALID,
-                "wave solve: missing inputs");
     int dev = 0;
     RRG_CUDA(cudaGetDevice(&dev));
     {
@@ -821,28 +832,24 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
         static bool done[64] = {};
         std::lock_guard<std::mutex> lock(mu);
         if (dev < 0 || dev >= 64 || !done[dev]) {
-            set_smem_attr<8, false>();
-            set_smem_attr<16, false>();
-            set_smem_attr<32, false>();
-            set_smem_attr<8, true>();
-            set_smem_attr<16, true>();
-            set_smem_attr<32, true>();
-            for (const void* k : {reinterpret_cast<const void*>(&wave_solve_tb_kernel<false>),
-                                  reinterpret_cast<const void*>(&wave_solve_tb_kernel<true>)})
-                RRG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              static_cast<int>(tb::smem)));
+            set_smem_attr<8>();
+            set_smem_attr<16>();
+            set_smem_attr<32>();
+            RRG_CUDA(cudaFuncSetAttribute(wave_solve_tb_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(tb::smem)));
             if (dev >= 0 && dev < 64) done[dev] = true;
         }
     }
     int per_sm = 0;
     if (tbk)
-        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, wave_solve_tb_kernel<false>, tb::T, tb::smem));
+        RRG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave_solve_tb_kernel,
+                                                               tb::T, tb::smem));
     else
         per_sm = W == 8 ? blocks_per_sm<8>() : (W == 16 ? blocks_per_sm<16>() : blocks_per_sm<32>());
     if (static_cast<int64_t>(per_sm) * num_sms(dev) < nblocks)
         return false;  // not all blocks could be resident at once
-    SolveArgs a{};
+    SolveArgs a;
     a.phi0 = phi0;
     a.phi1 = phi1;
     a.cur = cur;
@@ -852,14 +859,15 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
     a.inv_scale = ldexp(1.0, -shift_s);
     a.inv_dx3 = 1.0 / (dx * dx * dx);
     a.rho_sub = rho_sub;
-    a.src = src;
-    a.g = g;
-    a.d_old = d_old;
     a.km = static_cast<float>(w.K_MAIN);
     a.ka = static_cast<float>(w.K_ACTUAL);
     a.ko = static_cast<float>(w.K_OLD);
-    a.kf = inc ? 1.0f : static_cast<float>(w.K_F);
+    a.kf = 1.0f;
+    a.kf_d = w.K_F;
+    a.km_d = w.K_MAIN;
+    a.kao_d = w.K_ACTUAL + w.K_OLD - 1.0;
     a.grad_coef = static_cast<float>(-1.0 / dx);
+    a.src = src;
     a.acc4 = acc4;
     a.sync = sync;
     cudaLaunchConfig_t cfg = {};
@@ -874,20 +882,16 @@ bool launch_wave_solve(int nx, int iterations, float* phi0, float* phi1, int cur
     if (tbk) {
         cfg.blockDim = dim3(tb::T);
         cfg.dynamicSmemBytes = tb::smem;
-        if (inc) launch_coop(cfg, wave_solve_tb_kernel<true>, a);
-        else launch_coop(cfg, wave_solve_tb_kernel<false>, a);
+        RRG_CUDA(cudaLaunchKernelEx(&cfg, wave_solve_tb_kernel, a));
     } else if (W == 8) {
         cfg.dynamicSmemBytes = Shape<8>::smem;
-        if (inc) launch_coop(cfg, wave_solve_kernel<8, true>, a);
-        else launch_coop(cfg, wave_solve_kernel<8, false>, a);
+        RRG_CUDA(cudaLaunchKernelEx(&cfg, wave_solve_kernel<8>, a));
     } else if (W == 16) {
         cfg.dynamicSmemBytes = Shape<16>::smem;
-        if (inc) launch_coop(cfg, wave_solve_kernel<16, true>, a);
-        else launch_coop(cfg, wave_solve_kernel<16, false>, a);
+        RRG_CUDA(cudaLaunchKernelEx(&cfg, wave_solve_kernel<16>, a));
     } else {
         cfg.dynamicSmemBytes = Shape<32>::smem;
-        if (inc) launch_coop(cfg, wave_solve_kernel<32, true>, a);
-        else launch_coop(cfg, wave_solve_kernel<32, false>, a);
+        RRG_CUDA(cudaLaunchKernelEx(&cfg, wave_solve_kernel<32>, a));
     }
     RRG_LAUNCHED();
     return true;

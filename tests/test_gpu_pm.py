@@ -422,9 +422,9 @@ def test_persistent_wave_solve_equals_one_launch_per_substep(monkeypatch, prec, 
         np.testing.assert_array_equal(g1[k], g0[k])
     for a, b in zip(w1, w0):
         np.testing.assert_array_equal(a, b)
-    # after the same preparation, one kernel instead of the substeps, the finish and the
+    # one kernel instead of the increments' preparation, the substeps, the finish and the
     # gradient in each of the 9 steps
-    assert launches[0] + 9 * (iterations + 1) == launches[1]
+    assert launches[0] + 9 * (iterations + 2) == launches[1]
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])

@@ -186,14 +186,19 @@ def test_gpu_pm_matches_reference(name, prec):
     assert np.max(np.abs(gr["mass"] - g["mass0"])) <= 0.5 * 8 * n * 2.0 ** -shift
     scale = np.max(np.abs(g["phi0"]))
     assert np.max(np.abs(gr["grav"] - g["phi0"])) <= (1e-7 if prec == "fp64" else 1e-4) * scale
-    a_tol = 1e-6 if prec == "fp64" else 1e-3
+    # measured: precalc accelerations FP32 / MIXED 0.7e-6 .. 9.7e-6 (the steady FP32 relaxation
+    # carries its rounding times the lowest mode's conditioning), FP64 1.1e-9 .. 1.9e-9
+    a_tol = 1e-8 if prec == "fp64" else 3e-5
     e0 = float(np.median(rel_err(s0["acc"], g["acc0"])))
     print(f"\n{name} {prec}: precalc acc median rel err {e0:.3e}; after the steps: pos max "
           f"{np.max(np.abs(s['pos'] - g['pos_n'])):.3e}, vel median "
           f"{np.median(rel_err(s['vel'], g['vel_n'])):.3e}")
     assert e0 <= a_tol
-    assert np.max(np.abs(s["pos"] - g["pos_n"])) <= (1e-9 if prec == "fp64" else 1e-5)
-    assert np.median(rel_err(s["vel"], g["vel_n"])) <= (1e-6 if prec == "fp64" else 1e-4)
+    # measured after the steps: positions FP32 <= 1.0e-6, MIXED <= 2.4e-9, FP64 <= 2.8e-14;
+    # velocities (median) 6e-8 .. 8e-8 in FP32 / MIXED, <= 2.3e-12 in FP64
+    pos_tol = {"fp64": 1e-12, "mixed": 1e-8, "fp32": 3e-6}[prec]
+    assert np.max(np.abs(s["pos"] - g["pos_n"])) <= pos_tol
+    assert np.median(rel_err(s["vel"], g["vel_n"])) <= (1e-10 if prec == "fp64" else 3e-7)
 
 
 @pytest.mark.gpu

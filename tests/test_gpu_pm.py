@@ -238,17 +238,20 @@ def test_pm_steps_match_oracle(prec):
     st.solve(og, mgrid, 600)
     ra0 = orc.interp(pos, og, orc.gradient(og, st.curr))
     # the deposit is int64 fixed point in every precision (2^-27 relative per contribution),
-    # so even the FP64 path differs from the reference's FP64 atomics at the 1e-8 level
-    tol_a = 1e-6 if prec == "fp64" else 1e-4
+    # so even the FP64 path differs from the reference's FP64 atomics at the 1e-8 level.
+    # Measured: precalc accelerations FP32 / MIXED 2.2e-6 / 2.3e-6 (the relaxations differ by the
+    # steady state's FP32 rounding), FP64 3.4e-10; after 10 steps accelerations 1.1e-7 / 9.6e-8 /
+    # 3.6e-10, positions 4.8e-8 / 4.7e-10 / 2.6e-15, velocities 9.0e-8 / 9.0e-8 / 6.2e-13.
+    tol_a = 1e-8 if prec == "fp64" else 1e-5
     assert np.median(rel_err(a0, ra0)) <= tol_a
     rp, rv, ra = orc.pm_steps(pos, vel, ra0, m, og, 20, dt, st, steps)
     print(f"\n{prec}: precalc acc {np.median(rel_err(a0, ra0)):.3e}; after {steps} steps: acc "
           f"{np.median(rel_err(got['acc'], ra)):.3e}, pos {np.median(rel_err(got['pos'], rp)):.3e}, "
           f"vel {np.median(rel_err(got['vel'], rv)):.3e}")
-    assert np.median(rel_err(got["pos"], rp)) <= (1e-10 if prec == "fp64" else 1e-5)
+    assert np.median(rel_err(got["pos"], rp)) <= {"fp64": 1e-12, "mixed": 5e-9, "fp32": 3e-7}[prec]
     assert np.max(np.abs(got["pos"] - rp)) <= (1e-9 if prec == "fp64" else 2e-5)
-    assert np.median(rel_err(got["vel"], rv)) <= (1e-6 if prec == "fp64" else 1e-4)
-    assert np.median(rel_err(got["acc"], ra)) <= tol_a
+    assert np.median(rel_err(got["vel"], rv)) <= (1e-10 if prec == "fp64" else 1e-6)
+    assert np.median(rel_err(got["acc"], ra)) <= (1e-8 if prec == "fp64" else 1e-6)
 
 
 @pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])

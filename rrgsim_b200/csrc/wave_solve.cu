@@ -169,7 +169,23 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
     float4 cur[ZC], old[ZC];
 #pragma unroll
-    for (int k = 0; k < ZC; ++k) cur[k] = __ldcg(c4 + col + k * plane4);
+    for (int k = 0; k < ZC; ++k) {
+        cur[k] = __ldcg(c4 + col + k * plane4);
+        tile[(k * (RB + 2) + r + 1) * W + q] = cur[k];
+    }
+    // phi0's halo straight from global memory (rows y0 - 1 and y0 + RB at the own planes, planes
+    // z0 - 1 and z0 + ZC of the own rows, periodic): no exchange is needed for level 0
+    for (int i = tid; i < 2 * S::Hy; i += kThreads) {
+        const int reg = i / S::Hy, off = i - reg * S::Hy, k = off / W, qq = off - k * W;
+        const int yy = reg == 0 ? (y0 == 0 ? nx - 1 : y0 - 1) : (y0 + RB == nx ? 0 : y0 + RB);
+        tile[(k * (RB + 2) + (reg == 0 ? 0 : RB + 1)) * W + qq] =
+            __ldcg(c4 + (static_cast<size_t>(z0 + k) * nx + yy) * W + qq);
+    }
+    for (int i = tid; i < 2 * S::Hz; i += kThreads) {
+        const int reg = i / S::Hz, off = i - reg * S::Hz, rr = off / W, qq = off - rr * W;
+        const int zz = reg == 0 ? (z0 == 0 ? nx - 1 : z0 - 1) : (z0 + ZC == nx ? 0 : z0 + ZC);
+        zh[i] = __ldcg(c4 + (static_cast<size_t>(zz) * nx + y0 + rr) * W + qq);
+    }
     auto source = [&](size_t o4, double sd[4]) {
         const ulonglong2 m01 = __ldcg(m2 + 2 * o4);
         const ulonglong2 m23 = __ldcg(m2 + 2 * o4 + 1);
@@ -249,11 +265,9 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     };
 
     // ---- substeps --------------------------------------------------------------------------
-    const unsigned int e0 = base + 1;   // epoch of level 0; level t has e0 + t
-#pragma unroll
-    for (int k = 0; k < ZC; ++k) store_faces(e0, k, cur[k]);
-    publish(e0);
-    if (!exchange(e0)) return;
+    // level t + 1 is published as epoch e0 + t + 1 (level 0 is not exchanged)
+    const unsigned int e0 = base;
+    __syncthreads();  // phi0 and its halo in the tile
     // the increments' source g from phi0 and its halo (wave_inc_source); the plain source stored
     // where asked, the other deposit cleared; then level 0 of the increments is zero everywhere
     // and the one before it phi_prev - phi0
@@ -314,9 +328,9 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
         }
         const unsigned int e = e0 + t + 1;
         publish(e);  // (its barrier also ends this substep's reads of the tile and halo)
-        if (t + 1 < a.iterations || a.acc4 != nullptr) {
-            if (!exchange(e)) return;
-        }
+        // (the last exchange gives the gradient its halo; it also keeps every block's final
+        // writes after its neighbours' reads of phi0's halo, even without a gradient)
+        if (!exchange(e)) return;
     }
 
     // ---- the levels to global memory (only this thread reads them in this launch) ---------

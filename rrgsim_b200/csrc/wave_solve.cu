@@ -54,7 +54,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kZC = 8;                          // planes per block
-constexpr double kPiW = 3.14159265358979;       // the reference's PI (co_info_structs.h:7)
 constexpr long long kWaitCycles = 1ll << 28;    // ~0.14 s at 1.9 GHz per wait at most
 constexpr int kCounterStride = 32;              // a block's epoch counter: 128 bytes apart
 constexpr int kErrWord = 16383;                 // in the first 64 KB: counters, error word
@@ -376,11 +375,18 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
                 ez = make_float4(0.5f * (zp.x - zm.x), 0.5f * (zp.y - zm.y), 0.5f * (zp.z - zm.z),
                                  0.5f * (zp.w - zm.w));
             const float g = a.grad_coef;
-            float4* o = a.acc4 + (static_cast<size_t>(z) * nx + y) * nx + x;
-            o[0] = make_float4(d0 * g, ey.x * g, ez.x * g, c.x);
-            o[1] = make_float4(d1 * g, ey.y * g, ez.y * g, c.y);
-            o[2] = make_float4(d2 * g, ey.z * g, ez.z * g, c.z);
-            o[3] = make_float4(d3 * g, ey.w * g, ez.w * g, c.w);
+            // a warp's 128 cells are contiguous (its rows are consecutive): staged through the
+            // source area (idle now), then stored 512 contiguous bytes per instruction
+            float4* const st = srcs + (tid >> 5) * 128;
+            __syncwarp();
+            st[4 * lane] = make_float4(d0 * g, ey.x * g, ez.x * g, c.x);
+            st[4 * lane + 1] = make_float4(d1 * g, ey.y * g, ez.y * g, c.y);
+            st[4 * lane + 2] = make_float4(d2 * g, ey.z * g, ez.z * g, c.z);
+            st[4 * lane + 3] = make_float4(d3 * g, ey.w * g, ez.w * g, c.w);
+            __syncwarp();
+            float4* const o = a.acc4 + (static_cast<size_t>(z) * nx + (y - lane / W)) * nx;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[i * 32 + lane] = st[i * 32 + lane];
         }
     }
     // the counter ends at e0 + iterations in every block: the next launch starts from there
@@ -773,11 +779,18 @@ __global__ void __launch_bounds__(tb::T, 1) wave_solve_tb_kernel(const SolveArgs
                 ez = make_float4(0.5f * (zp.x - zm.x), 0.5f * (zp.y - zm.y), 0.5f * (zp.z - zm.z),
                                  0.5f * (zp.w - zm.w));
             const float g = a.grad_coef;
-            float4* o = a.acc4 + (static_cast<size_t>(z) * NX + y) * NX + x;
-            o[0] = make_float4(d0 * g, ey.x * g, ez.x * g, c.x);
-            o[1] = make_float4(d1 * g, ey.y * g, ez.y * g, c.y);
-            o[2] = make_float4(d2 * g, ey.z * g, ez.z * g, c.z);
-            o[3] = make_float4(d3 * g, ey.w * g, ez.w * g, c.w);
+            // the warp's row (128 cells) staged through the source area (idle now), then stored
+            // 512 contiguous bytes per instruction
+            float4* const st = srcs + warp * 128;
+            __syncwarp();
+            st[4 * lane] = make_float4(d0 * g, ey.x * g, ez.x * g, c.x);
+            st[4 * lane + 1] = make_float4(d1 * g, ey.y * g, ez.y * g, c.y);
+            st[4 * lane + 2] = make_float4(d2 * g, ey.z * g, ez.z * g, c.z);
+            st[4 * lane + 3] = make_float4(d3 * g, ey.w * g, ez.w * g, c.w);
+            __syncwarp();
+            float4* const o = a.acc4 + (static_cast<size_t>(z) * NX + y) * NX;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[i * 32 + lane] = st[i * 32 + lane];
         }
     }
     // the counter ends at base + (passes) in every block: the next launch starts from there

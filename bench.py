@@ -341,10 +341,13 @@ def run_native(args):
     step_bytes = 52 * N_PART + (20 * 16 + 16 + 12) * cells
     hbm, how, pk = peaks()
     achieved = alg_bytes / (solve_ms * 1e-3) / 1e9
+    # the 128^3 solve runs wave_solve_kernel, or wave_solve_tb_kernel under RRG_WAVE_TB=1
+    solve_kernel = ("wave_solve_tb_kernel" if os.environ.get("RRG_WAVE_TB", "0") not in ("", "0")
+                    else "wave_solve_kernel")
     traffic = None
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("wave_solve_kernel_bytes_per_launch")
+        traffic = json.loads(tf.read_text()).get(f"{solve_kernel}_bytes_per_launch")
     # the per-substep stencil of the operator path (solve_wave_equation), for comparison: its
     # algorithmic bytes are 16 B/cell (read phi, phi_old, src; write phi_new)
     ctx.solve_wave_equation(8)
@@ -492,7 +495,7 @@ def run_native(args):
                     "d2h_bytes_per_step": d2h, "steps": k_e2e, "statistic": "median of 7 runs",
                     "runs": [N_PART * k_e2e * world / t for t in e2e_runs]},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "wave_solve_kernel", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": solve_kernel, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_kind": how,
                          "ms_per_launch": solve_ms, "alg_bytes_per_launch": alg_bytes,

@@ -122,6 +122,10 @@ void launch_wave_source(int prec, int nx, const unsigned long long* mgrid, int s
 // If maxbits != nullptr also folds max|phi_new - phi| and max|phi_new| into maxbits[0..1].
 void launch_wave_step(int prec, int nx, const void* phi, void* phi_old_inout, const void* src,
                       const WaveCoef& c, unsigned long long* maxbits, cudaStream_t s);
+// One adjoint substep of the PM adjoint on a periodic FP32 grid with the float4 stencil:
+// P <- km L6(C) + ka C + beta P, F += kf C. False (nothing launched) where the rows do not tile.
+bool launch_wave_adjoint_step(int nx, const float* C, float* P, float* F, double km, double ka,
+                              double beta, double kf, cudaStream_t s);
 // a = -grad phi on the grid (rm_p2mesh.cu:238-290): acc4[c] = (ax, ay, az, phi[c]).
 void launch_gradient(int prec, int nx, double dx, const void* phi, void* acc4, cudaStream_t s);
 // One damped-wave update of four x-cells (wave_diss_iteration, wave.cu:106-193, periodic box,

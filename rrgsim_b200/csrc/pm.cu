@@ -426,10 +426,12 @@ __global__ void __launch_bounds__(kTX* kTY, 8) wave_periodic_kernel(
 // planes. About 1.5 memory instructions per cell instead of 7. Same arithmetic as
 // wave_periodic_kernel: lap = x- + x+ + y- + y+ + z- + z+, out = lap K_MAIN + phi K_ACTUAL +
 // phi_old K_OLD + src K_F.
-template <int ZC, bool CHECK, int BS>
+// ADJ: the adjoint substep of the PM adjoint instead (phi the current cotangent C, phi_old the
+// previous one P, no source): P <- K_MAIN L6(C) + K_ACTUAL C + K_OLD P and F += K_F C.
+template <int ZC, bool CHECK, int BS, bool ADJ = false>
 __global__ void __launch_bounds__(BS, 1024 / BS) wave_periodic_x4_kernel(
     const float* __restrict__ phi, float* __restrict__ phi_old, const float* __restrict__ src,
-    const WaveDev w, unsigned long long* __restrict__ maxbits) {
+    const WaveDev w, unsigned long long* __restrict__ maxbits, float* __restrict__ fadj = nullptr) {
     const int nx = w.nx;
     const int W = nx >> 2;       // float4 per row
     const int plane4 = W * nx;   // float4 per plane
@@ -484,6 +486,17 @@ __global__ void __launch_bounds__(BS, 1024 / BS) wave_periodic_x4_kernel(
             const float4 yp = __ldg(phi4 + gyp + z * plane4);
             const float4 zm = pv[k], zp = pv[k + 2];
             const float4 po = old4[o];
+            if constexpr (ADJ) {
+                old4[o] = wave_cell4(c, lft, rgt, ym, yp, zm, zp, po, zero4, km, ka, ko, 0.f);
+                float4* f4 = reinterpret_cast<float4*>(fadj) + o;
+                float4 f = *f4;
+                f.x = __fmaf_rn(kf, c.x, f.x);
+                f.y = __fmaf_rn(kf, c.y, f.y);
+                f.z = __fmaf_rn(kf, c.z, f.z);
+                f.w = __fmaf_rn(kf, c.w, f.w);
+                *f4 = f;
+                continue;
+            }
             const float4 s = __ldg(src4 + o);
             const float4 out = wave_cell4(c, lft, rgt, ym, yp, zm, zp, po, s, km, ka, ko, kf);
             old4[o] = out;
@@ -993,6 +1006,27 @@ void launch_wave_inc_finish(int nx, const float* phi0, const float* d_fin, const
     const int64_t nc = static_cast<int64_t>(nx) * nx * nx;
     wave_inc_finish_kernel<<<div_up(nc, 256), 256, 0, s>>>(nc, phi0, d_fin, d_prv, fin, prv);
     RRG_LAUNCHED();
+}
+
+// One adjoint substep of the PM adjoint with the float4 stencil (FP32, periodic): false,
+// launching nothing, on grids whose rows do not tile into warps.
+bool launch_wave_adjoint_step(int nx, const float* C, float* P, float* F, double km, double ka,
+                              double beta, double kf, cudaStream_t s) {
+    const int W4 = nx / 4;
+    if (nx < 16 || nx % 8 != 0 || !(32 % W4 == 0 || W4 % 32 == 0)) return false;
+    WaveDev w{};
+    w.nx = nx;
+    w.uniform = 1;
+    w.bc = RRG_BC_PERIODIC;
+    w.K_MAIN = km;
+    w.K_ACTUAL = ka;
+    w.K_OLD = beta;
+    w.K_F = kf;
+    const int bs = 128;
+    dim3 g4(div_up(static_cast<int64_t>(W4) * nx, bs), nx / 8);
+    wave_periodic_x4_kernel<8, false, 128, true><<<g4, bs, 0, s>>>(C, P, nullptr, w, nullptr, F);
+    RRG_LAUNCHED();
+    return true;
 }
 
 // RRG_WAVE_BS = 128 / 256 fixes the block size of the float4 stencil (for sweeps).

@@ -338,11 +338,20 @@ void backward_step(rrg_pm_adjoint* P, const void* xn1, const void* phin1, cudaSt
     RRG_CUDA(cudaMemsetAsync(P->F.p, 0, P->F.bytes, s));
     R beta = R(1);
     for (int k = 0; k < P->substeps; ++k) {
-        wave_adjoint_kernel<R><<<bg, 256, 0, s>>>(
-            P->grid.nx, static_cast<const R*>(P->Cb.p), static_cast<R*>(P->Pb.p),
-            static_cast<R*>(P->F.p), static_cast<R>(P->wc.K_MAIN), static_cast<R>(P->wc.K_ACTUAL),
-            beta, static_cast<R>(P->wc.K_F));
-        RRG_LAUNCHED();
+        // FP32: the float4 stencil (x +- 1 by shuffles, z from a register pipeline)
+        const bool x4 = sizeof(R) == 4 &&
+                        launch_wave_adjoint_step(P->grid.nx, static_cast<const float*>(P->Cb.p),
+                                                 static_cast<float*>(P->Pb.p),
+                                                 static_cast<float*>(P->F.p), P->wc.K_MAIN,
+                                                 P->wc.K_ACTUAL, static_cast<double>(beta),
+                                                 P->wc.K_F, s);
+        if (!x4) {
+            wave_adjoint_kernel<R><<<bg, 256, 0, s>>>(
+                P->grid.nx, static_cast<const R*>(P->Cb.p), static_cast<R*>(P->Pb.p),
+                static_cast<R*>(P->F.p), static_cast<R>(P->wc.K_MAIN),
+                static_cast<R>(P->wc.K_ACTUAL), beta, static_cast<R>(P->wc.K_F));
+            RRG_LAUNCHED();
+        }
         std::swap(P->Cb.p, P->Pb.p);  // the new current cotangent; old C becomes P / K_O
         beta = static_cast<R>(P->wc.K_OLD);
     }

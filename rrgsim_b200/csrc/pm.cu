@@ -1022,9 +1022,26 @@ bool launch_wave_adjoint_step(int nx, const float* C, float* P, float* F, double
     w.K_ACTUAL = ka;
     w.K_OLD = beta;
     w.K_F = kf;
+    // z-chunk as the forward stencil chooses it: the longest of 8, 4, 2 planes that still gives
+    // two 256-thread blocks' worth of threads per SM
+    int dev = 0;
+    RRG_CUDA(cudaGetDevice(&dev));
+    const int sms = num_sms(dev);
     const int bs = 128;
-    dim3 g4(div_up(static_cast<int64_t>(W4) * nx, bs), nx / 8);
-    wave_periodic_x4_kernel<8, false, 128, true><<<g4, bs, 0, s>>>(C, P, nullptr, w, nullptr, F);
+    const int rows_blocks = div_up(static_cast<int64_t>(W4) * nx, bs);
+    int zx = 2;
+    for (int cand : {8, 4})
+        if (static_cast<int64_t>(rows_blocks) * (nx / cand) * bs >= 2 * 256 * sms) {
+            zx = cand;
+            break;
+        }
+    const dim3 g4(rows_blocks, nx / zx);
+    if (zx == 8)
+        wave_periodic_x4_kernel<8, false, 128, true><<<g4, bs, 0, s>>>(C, P, nullptr, w, nullptr, F);
+    else if (zx == 4)
+        wave_periodic_x4_kernel<4, false, 128, true><<<g4, bs, 0, s>>>(C, P, nullptr, w, nullptr, F);
+    else
+        wave_periodic_x4_kernel<2, false, 128, true><<<g4, bs, 0, s>>>(C, P, nullptr, w, nullptr, F);
     RRG_LAUNCHED();
     return true;
 }

@@ -370,6 +370,9 @@ def run_native(args):
            for k, v in dict(pos=pos, vel=vel, mass=mass, soft2=soft2).items()}
     ctx2.init_grid(grid)
     ctx2.set_wave_params(wave)
+    # each step's last particle pass also forms the conservation sums, which the per-step
+    # diagnostics read then only combine
+    ctx2.set_step_sums(True)
     if args.sort_interval is not None:
         ctx2.set_sort_interval(args.sort_interval)
     ctx2.load_particles(pin["pos"], pin["vel"], pin["mass"], pin["soft2"])

@@ -313,6 +313,16 @@ RRG_API rrg_status rrg_set_wave_state(rrg_ctx* ctx, const double* phi_cur,
  * not depend on the interval. */
 RRG_API rrg_status rrg_set_sort_interval(rrg_ctx* ctx, int interval);
 
+/* enable != 0: in wave mode the last particle pass of every rrg_solver_calc_steps call also
+ * forms the conservation sums of the state it leaves (8 double-doubles per 256 particles), so
+ * that rrg_calc_conservation / rrg_calc_conservation_async right after the call only combine
+ * them (one small kernel) instead of reading every particle again. Any other call that may
+ * change the state in between makes them recompute from the particles. The sums are the same
+ * double-double reductions either way. Off by default: it costs the pass a little when no
+ * diagnostics follow. No reference counterpart (calc_conservation, nbody.cu:246-291, always
+ * reads the particles). */
+RRG_API rrg_status rrg_set_step_sums(rrg_ctx* ctx, int enable);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Host I/O — the rrgsim executable's boundary (no GPU needed)                                 */
 /* ------------------------------------------------------------------------------------------ */

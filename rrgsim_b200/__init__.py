@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "rrg_get_wave_state": (st, [vp, d, d]),
         "rrg_set_wave_state": (st, [vp, d, d]),
         "rrg_set_sort_interval": (st, [vp, i32]),
+        "rrg_set_step_sums": (st, [vp, i32]),
         "rrg_parse_params_json": (st, [C.c_char_p, C.POINTER(ParsedParams)]),
         "rrg_read_ic_component": (st, [C.c_char_p, C.c_double, C.c_double, i64, i64, d, d, d, d,
                                        C.POINTER(i64)]),
@@ -406,6 +407,11 @@ class Context:
 
     def set_sort_interval(self, interval: int) -> None:
         self._c(lib().rrg_set_sort_interval(self._h, int(interval)))
+
+    def set_step_sums(self, enable: bool) -> None:
+        """Wave mode: the last particle pass of each calc_steps call also forms the
+        conservation sums, so a calc_conservation(_async) right after it only combines them."""
+        self._c(lib().rrg_set_step_sums(self._h, 1 if enable else 0))
 
 
 class Ensemble:

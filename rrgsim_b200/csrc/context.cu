@@ -129,6 +129,12 @@ struct rrg_ctx {
     // reductions / transfers
     Buf red_partial, red_out, dl, chk;
     double* host_red = nullptr;
+    // rrg_set_step_sums: the last particle pass of each fused chunk also writes the conservation
+    // sums' block records (step_partial); sums_ready says they describe the current state (every
+    // entry point clears it unless it leaves the state as it found it)
+    bool step_sums = false;
+    mutable bool sums_ready = false;
+    Buf step_partial;
 
     // solver
     bool solver_ready = false;
@@ -145,7 +151,7 @@ struct rrg_ctx {
     int64_t steps_since_sort = INT64_MAX / 2;
     Buf sort_keys, sort_dest, sort_counts, sort_offsets, sort_cursor, sort_temp, sort_stage;
     size_t sort_temp_bytes = 0;
-    std::map<std::tuple<int, int, int, int, bool>, GraphExec> graphs;
+    std::map<std::tuple<int, int, int, int, bool, bool>, GraphExec> graphs;
 
     ~rrg_ctx() {
         for (auto& kv : graphs)
@@ -165,6 +171,9 @@ namespace {
     try {                                                                                     \
         RRG_REQUIRE((ctx) != nullptr, RRG_ERR_INVALID, "null context");                       \
         RRG_CUDA(cudaSetDevice((ctx)->device));                                               \
+        const bool entry_sums_ready = (ctx)->sums_ready;                                      \
+        (ctx)->sums_ready = false;                                                            \
+        (void)entry_sums_ready;                                                               \
         __VA_ARGS__;                                                                          \
         return RRG_OK;                                                                        \
     } catch (const Error& e) {                                                                \
@@ -350,7 +359,18 @@ PmParticleArgs pm_args(rrg_ctx* c, int deposit_target) {
     a.shift_s = c->shift_s;
     a.mgrid = deposit_target >= 0 ? c->mg[deposit_target].as<unsigned long long>() : nullptr;
     a.dt = c->sim.dt_dynamics;
+    a.pot = c->pot.p;
+    a.partial = c->step_partial.as<double>();
     return a;
+}
+
+// Block records of the particle pass's conservation sums (PM_SUMS): 8 double-doubles per
+// block of kPmThreads particles.
+int step_sum_blocks(const rrg_ctx* c) { return div_up(c->n, kPmThreads); }
+void alloc_step_partial(rrg_ctx* c) {
+    if (c->step_sums && c->n > 0)
+        c->step_partial.alloc(static_cast<size_t>(step_sum_blocks(c)) * kPmSumValues * 2 *
+                              sizeof(double));
 }
 
 // Steady-state controlled relaxation (solve_wave_equation, wave.cu:230-297). Host-synchronous
@@ -537,7 +557,8 @@ void record_wave_steps(rrg_ctx* c, int nsteps, bool prologue) {
             PmParticleArgs a = pm_args(c, 1 - c->mg_cur);  // zeroed by this step's source pass
             a.pos_out = c->posm[1 - c->cur].p;
             a.lo_out = c->prec == RRG_PREC_MIXED ? c->poslo[1 - c->cur].p : nullptr;
-            launch_pm_particles(a, PM_INTERP_CORRECT | PM_WRITE_SYNC | PM_PREDICT_DEPOSIT,
+            launch_pm_particles(a, PM_INTERP_CORRECT | PM_WRITE_SYNC | PM_PREDICT_DEPOSIT |
+                                       (c->step_sums ? PM_SUMS : 0),
                                 c->stream);
         }
     }
@@ -568,7 +589,8 @@ GraphExec& chunk_graph(rrg_ctx* c, int nsteps) {
         c->pending = false;
         prologue = false;
     }
-    const auto key = std::make_tuple(nsteps, c->cur, c->mg_cur, c->phi_cur, prologue);
+    const bool sums = c->wave_mode && c->step_sums;
+    const auto key = std::make_tuple(nsteps, c->cur, c->mg_cur, c->phi_cur, prologue, sums);
     auto it = c->graphs.find(key);
     const int cur0 = c->cur, mg0 = c->mg_cur, phi0 = c->phi_cur;
     if (it == c->graphs.end()) {
@@ -730,6 +752,7 @@ RRG_API rrg_status rrg_synchronize(rrg_ctx* ctx) {
     RRG_ENTRY(ctx, {
         RRG_CUDA(cudaStreamSynchronize(ctx->stream));
         check_wave_solve(ctx);
+        ctx->sums_ready = entry_sums_ready;
     })
 }
 
@@ -795,7 +818,8 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         const auto layout = [&]() {
             return std::vector<const void*>{ctx->posm[0].p, ctx->posm[1].p, ctx->poslo[0].p,
                                             ctx->poslo[1].p, ctx->vel.p, ctx->acc.p, ctx->u.p,
-                                            ctx->pot.p, ctx->hsoft.p, ctx->scratch.p};
+                                            ctx->pot.p, ctx->hsoft.p, ctx->scratch.p,
+                                            ctx->step_partial.p};
         };
         const auto before = layout();
         const int64_t n_before = ctx->n;
@@ -832,7 +856,8 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         ctx->pot.alloc(ctx->rsz * n);
         if (!uniform) ctx->hsoft.alloc(ctx->rsz * n);
         else ctx->hsoft.release();
-        ctx->id.release();
+        // the id buffer stays allocated (its contents are rewritten by the first sort); freeing
+        // and allocating it again on every reload cost the host two synchronous driver calls
         ctx->steps_since_sort = INT64_MAX / 2;
         ctx->splits = direct_choose_splits(ctx->prec, n, ctx->sms);
         const size_t sb = direct_scratch_bytes(ctx->prec, n, ctx->splits);
@@ -840,6 +865,7 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         const int rb = conservation_blocks(n);
         ctx->red_partial.alloc(static_cast<size_t>(rb) * 12 * 2 * sizeof(double));  // (hi, lo)
         ctx->red_out.alloc(16 * sizeof(double));
+        alloc_step_partial(ctx);
         if (layout() != before || n != n_before || ctx->shift_s != shift_before ||
             ctx->uniform_hsoft != hsoft_before || ctx->soft_uniform != uniform_before)
             drop_graphs(ctx);
@@ -851,7 +877,8 @@ RRG_API rrg_status rrg_load_particles(rrg_ctx* ctx, int64_t n, const double* pos
         RRG_CUDA(cudaMemsetAsync(ctx->acc.p, 0, vb, ctx->stream));
         RRG_CUDA(cudaMemsetAsync(ctx->u.p, 0, vb, ctx->stream));
         RRG_CUDA(cudaMemsetAsync(ctx->pot.p, 0, ctx->rsz * n, ctx->stream));
-        RRG_CUDA(cudaStreamSynchronize(ctx->stream));
+        // no wait: the host arrays were copied before the checks, and the packing kernels run
+        // ahead of whatever the caller enqueues next on the context stream
     })
 }
 
@@ -877,6 +904,7 @@ RRG_API rrg_status rrg_get_particles(rrg_ctx* ctx, double* pos, double* vel, dou
             RRG_CUDA(cudaMemcpyAsync(grav, d + 9 * n, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
         RRG_CUDA(cudaStreamSynchronize(ctx->stream));
         check_wave_solve(ctx);
+        ctx->sums_ready = entry_sums_ready;
     })
 }
 
@@ -980,6 +1008,7 @@ RRG_API rrg_status rrg_get_grid(rrg_ctx* ctx, double* mass, double* grav, double
                 }
             }
         }
+        ctx->sums_ready = entry_sums_ready;
     })
 }
 
@@ -1154,11 +1183,23 @@ RRG_API rrg_status rrg_project_grid_grav_on_particles(rrg_ctx* ctx) {
     })
 }
 
-static void reduce_state(rrg_ctx* ctx, bool com) {
-    const int rb = conservation_blocks(ctx->n);
-    launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
-                        ctx->red_partial.as<double>(), rb, ctx->red_out.as<double>(),
-                        ctx->stream, com);
+// The 12 sums of the current state into `out` (device-addressable): from the block records the
+// last fused particle pass left when they still describe the state (`ready`), else by a pass
+// over the particles.
+static void conservation_sums(rrg_ctx* ctx, bool com, bool ready, double* out) {
+    if (ready && !com) {
+        launch_conservation_finish_value_major(ctx->step_partial.as<double>(),
+                                               step_sum_blocks(ctx), kPmSumValues, out,
+                                               ctx->stream);
+    } else {
+        launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
+                            ctx->red_partial.as<double>(), conservation_blocks(ctx->n), out,
+                            ctx->stream, com);
+    }
+}
+
+static void reduce_state(rrg_ctx* ctx, bool com, bool ready) {
+    conservation_sums(ctx, com, ready, ctx->red_out.as<double>());
     RRG_CUDA(cudaMemcpyAsync(ctx->host_red, ctx->red_out.p, 12 * sizeof(double),
                              cudaMemcpyDeviceToHost, ctx->stream));
     RRG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1169,7 +1210,8 @@ RRG_API rrg_status rrg_calc_conservation(rrg_ctx* ctx, rrg_conservation* out) {
     RRG_ENTRY(ctx, {
         require_particles(ctx);
         RRG_REQUIRE(out != nullptr, RRG_ERR_INVALID, "NULL output");
-        reduce_state(ctx, false);
+        reduce_state(ctx, false, entry_sums_ready);
+        ctx->sums_ready = entry_sums_ready;
         const double* r = ctx->host_red;
         out->time = ctx->time;
         out->Ek = 0.5 * r[0];
@@ -1185,7 +1227,6 @@ RRG_API rrg_status rrg_calc_conservation_async(rrg_ctx* ctx, double* sums) {
     RRG_ENTRY(ctx, {
         require_particles(ctx);
         RRG_REQUIRE(sums != nullptr, RRG_ERR_INVALID, "NULL output");
-        const int rb = conservation_blocks(ctx->n);
         // pinned host memory that this device can address takes the sums straight from the
         // finishing kernel: no copy-engine hop between the step's kernels
         double* out = ctx->red_out.as<double>();
@@ -1198,11 +1239,11 @@ RRG_API rrg_status rrg_calc_conservation_async(rrg_ctx* ctx, double* sums) {
         } else {
             (void)cudaGetLastError();
         }
-        launch_conservation(ctx->prec, ctx->n, ctx->P(), ctx->L(), ctx->vel.p, ctx->pot.p,
-                            ctx->red_partial.as<double>(), rb, out, ctx->stream, false);
+        conservation_sums(ctx, false, entry_sums_ready, out);
         if (!direct)
             RRG_CUDA(cudaMemcpyAsync(sums, ctx->red_out.p, 12 * sizeof(double),
                                      cudaMemcpyDeviceToHost, ctx->stream));
+        ctx->sums_ready = entry_sums_ready;
     })
 }
 
@@ -1223,7 +1264,8 @@ RRG_API rrg_status rrg_calc_mass_center(rrg_ctx* ctx, double center_of_mass[3],
                                         double* total_mass) {
     RRG_ENTRY(ctx, {
         require_particles(ctx);
-        reduce_state(ctx, true);
+        reduce_state(ctx, true, false);
+        ctx->sums_ready = entry_sums_ready;
         const double* r = ctx->host_red;
         const double M = r[8];
         for (int k = 0; k < 3; ++k)
@@ -1323,6 +1365,7 @@ RRG_API rrg_status rrg_get_wave_state(rrg_ctx* ctx, double* phi_cur, double* phi
         RRG_CUDA(cudaStreamSynchronize(ctx->stream));
         copy_level(ctx, ctx->phi[ctx->phi_cur].p, phi_cur, nullptr);
         copy_level(ctx, ctx->phi[1 - ctx->phi_cur].p, phi_prev, nullptr);
+        ctx->sums_ready = entry_sums_ready;
     })
 }
 
@@ -1356,6 +1399,8 @@ RRG_API rrg_status rrg_solver_calc_steps(rrg_ctx* ctx, int nsteps) {
                     if (sort) sort_particles(ctx);  // (a pending prediction is permuted along)
                     run_graph(ctx, chunk);
                 });
+                // the last chunk's last particle pass left the synced state's sums
+                ctx->sums_ready = ctx->wave_mode && ctx->step_sums;
             }
             for (int s = 0; s < nsteps; ++s) {
                 ctx->iter += 1;
@@ -1428,6 +1473,14 @@ RRG_API rrg_status rrg_set_sort_interval(rrg_ctx* ctx, int interval) {
     RRG_ENTRY(ctx, {
         RRG_REQUIRE(interval >= 0, RRG_ERR_INVALID, "interval must be >= 0");
         ctx->sort_interval = interval;
+        ctx->sums_ready = entry_sums_ready;
+    })
+}
+
+RRG_API rrg_status rrg_set_step_sums(rrg_ctx* ctx, int enable) {
+    RRG_ENTRY(ctx, {
+        ctx->step_sums = enable != 0;
+        alloc_step_partial(ctx);
     })
 }
 

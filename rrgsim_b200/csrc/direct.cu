@@ -376,6 +376,127 @@ __global__ void __launch_bounds__(kBS, 2) direct_f32x2_kernel(const F32Params p)
     }
 }
 
+// Paired over j (variants 6 and 7): each thread holds G i-particles, and each f32x2 instruction
+// takes one i against two consecutive j of the tile. One pair of shared-memory loads then feeds
+// G x 2 pairs with G = 1 already (the i-paired kernel needs G = 2 for that, and so half as many
+// blocks), and a block covers kBS x G particles. Shared layout per j-pair q:
+// (x_2q, x_2q+1, y_2q, y_2q+1), (z_2q, z_2q+1, m_2q, m_2q+1), (h_2q, h_2q+1); each thread's two
+// lanes (even and odd j) add at the end.
+template <int G, bool USOFT, bool POT, bool UMASS>
+__global__ void __launch_bounds__(kBS, 2) direct_f32jp_kernel(const F32Params p) {
+    __shared__ float4 s_xy[kBS / 2];
+    __shared__ float4 s_zm[kBS / 2];
+    __shared__ float2 s_h[USOFT ? 1 : kBS / 2];
+    const int tid = threadIdx.x;
+    const int64_t n = p.n;
+    const int64_t ibase = static_cast<int64_t>(blockIdx.x) * (kBS * G);
+
+    float2 nx[G], ny[G], nz[G], hs[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int64_t i = ibase + g * kBS + tid;
+        V4<float> pi = v4<float>(0.f, 0.f, 0.f, 0.f);
+        float h = p.uniform_h;
+        if (i < n) {
+            pi = p.posm[i];
+            if constexpr (!USOFT) h = p.hsoft[i];
+        }
+        nx[g] = make_float2(-pi.x, -pi.x);
+        ny[g] = make_float2(-pi.y, -pi.y);
+        nz[g] = make_float2(-pi.z, -pi.z);
+        hs[g] = USOFT ? make_float2(2.f * p.uniform_h, 2.f * p.uniform_h) : make_float2(h, h);
+    }
+    float2 ax[G], ay[G], az[G], ap[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) ax[g] = ay[g] = az[g] = ap[g] = make_float2(0.f, 0.f);
+
+    const int64_t jb = static_cast<int64_t>(blockIdx.y) * p.jchunk;
+    const int64_t je = min(n, jb + p.jchunk);
+    V4<float> nxt = v4<float>(kPadPos, kPadPos, kPadPos, 0.f);
+    float nxt_h = 1.f;
+    {
+        const int64_t j = jb + tid;
+        if (j < je) {
+            nxt = p.posm[j];
+            if constexpr (!USOFT) nxt_h = p.hsoft[j];
+        }
+    }
+    float* const fxy = reinterpret_cast<float*>(s_xy);
+    float* const fzm = reinterpret_cast<float*>(s_zm);
+    float* const fh = reinterpret_cast<float*>(s_h);
+    const int q0 = tid >> 1, e0 = tid & 1;
+    for (int64_t j0 = jb; j0 < je; j0 += kBS) {
+        __syncthreads();
+        fxy[4 * q0 + e0] = nxt.x;
+        fxy[4 * q0 + 2 + e0] = nxt.y;
+        fzm[4 * q0 + e0] = nxt.z;
+        fzm[4 * q0 + 2 + e0] = nxt.w;
+        if constexpr (!USOFT) fh[2 * q0 + e0] = nxt_h;
+        __syncthreads();
+        {
+            const int64_t j = j0 + kBS + tid;
+            nxt = v4<float>(kPadPos, kPadPos, kPadPos, 0.f);
+            nxt_h = 1.f;
+            if (j < je) {
+                nxt = p.posm[j];
+                if constexpr (!USOFT) nxt_h = p.hsoft[j];
+            }
+        }
+        float2 tx[G], ty[G], tz[G], tp[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) tx[g] = ty[g] = tz[g] = tp[g] = make_float2(0.f, 0.f);
+#pragma unroll 8
+        for (int q = 0; q < kBS / 2; ++q) {
+            const float4 xy = s_xy[q];
+            const float4 zm = s_zm[q];
+            const float2 px = make_float2(xy.x, xy.y), py = make_float2(xy.z, xy.w);
+            const float2 pz = make_float2(zm.x, zm.y), pm = make_float2(zm.z, zm.w);
+            float2 hj = make_float2(0.f, 0.f);
+            if constexpr (!USOFT) hj = s_h[q];
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const float2 dx = __fadd2_rn(px, nx[g]);
+                const float2 dy = __fadd2_rn(py, ny[g]);
+                const float2 dz = __fadd2_rn(pz, nz[g]);
+                const float2 s = USOFT ? hs[g] : __fadd2_rn(hs[g], hj);
+                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, s)));
+                const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
+                const float2 minv = UMASS ? inv : __fmul2_rn(pm, inv);
+                const float2 kk = __fmul2_rn(minv, __fmul2_rn(inv, inv));
+                tx[g] = __ffma2_rn(dx, kk, tx[g]);
+                ty[g] = __ffma2_rn(dy, kk, ty[g]);
+                tz[g] = __ffma2_rn(dz, kk, tz[g]);
+                if constexpr (POT) tp[g] = __fadd2_rn(tp[g], minv);
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            ax[g] = __fadd2_rn(ax[g], tx[g]);
+            ay[g] = __fadd2_rn(ay[g], ty[g]);
+            az[g] = __fadd2_rn(az[g], tz[g]);
+            if constexpr (POT) ap[g] = __fadd2_rn(ap[g], tp[g]);
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int64_t i = ibase + g * kBS + tid;
+        if (i >= n) continue;
+        float fx = ax[g].x + ax[g].y, fy = ay[g].x + ay[g].y, fz = az[g].x + az[g].y,
+              fp = ap[g].x + ap[g].y;
+        if constexpr (UMASS) {
+            fx *= p.uniform_m;
+            fy *= p.uniform_m;
+            fz *= p.uniform_m;
+            fp *= p.uniform_m;
+        }
+        if (gridDim.y > 1) {
+            p.part_hi[static_cast<int64_t>(blockIdx.y) * n + i] = v4<float>(fx, fy, fz, fp);
+        } else {
+            apply_epi<float, false>(p.epi, i, fx, fy, fz, -fp, POT, p.posm, p.poslo);
+        }
+    }
+}
+
 // Fixed-order FP64 reduction of the split partials, then the epilogue.
 template <bool MIXED>
 __global__ void direct_f32_finish(const F32Params p, int splits) {
@@ -490,8 +611,8 @@ void dispatch_f32(bool usoft, bool mixed, bool pot, dim3 grid, const F32Params& 
 
 // Kernel variants of the FP32 path: 1 = scalar, 1 i per thread; 2 = scalar, 2 i per thread;
 // 3 = paired f32x2, 2 i per thread; 4 = paired f32x2, 4 i per thread; 5 = paired f32x2, 6 i
-// per thread. MIXED and FP64 use the
-// scalar kernels. RRG_DIRECT_VARIANT overrides the choice (for sweeps).
+// per thread; 6 = paired over j, 1 i per thread; 7 = paired over j, 2 i per thread. MIXED and
+// FP64 use the scalar kernels. RRG_DIRECT_VARIANT overrides the choice (for sweeps).
 int env_variant() {
     static const int v = [] {
         const char* e = std::getenv("RRG_DIRECT_VARIANT");
@@ -504,19 +625,22 @@ int variant_for(int prec, int64_t n) {
     if (prec == RRG_PREC_FP64) return 1;
     const int e = env_variant();
     if (prec == RRG_PREC_MIXED) return (e == 1 || e == 2) ? e : (n <= 16384 ? 1 : 2);
-    if (e >= 1 && e <= 5) return e;
-    // measured on B200 (Plummer, FP32): the paired kernels lead from N = 16k on; 4 i-particles
-    // per thread pay off once there are enough blocks to fill the machine
-    return n < 131072 ? 3 : 4;
+    if (e >= 1 && e <= 7) return e;
+    // measured on B200 (Plummer, FP32, Gpairs/s at N = 16,384 / 65,536 / 262,144): paired
+    // over i with 2 i-particles per thread 2220 / 2588 / 2607, with 4: 2057 / 2478 / 2669;
+    // paired over j with 1: 2255 / 2672 / 2686, with 2: 2372 / 2722 / 2741
+    return n < 16384 ? 3 : 7;
 }
 
-int ipt_of(int variant) { return variant == 1 ? 1 : variant == 4 ? 4 : variant == 5 ? 6 : 2; }
+int ipt_of(int variant) {
+    return variant == 1 || variant == 6 ? 1 : variant == 4 ? 4 : variant == 5 ? 6 : 2;
+}
 
 int ipt_for(int prec, int64_t n) { return ipt_of(variant_for(prec, n)); }
 
 // Resident 256-thread blocks per SM of the kernel a variant launches (queried once).
 int resident_blocks(int prec, int variant) {
-    static int cache[3][6] = {};
+    static int cache[3][8] = {};
     int& r = cache[prec][variant];
     if (r) return r;
     const void* k = nullptr;
@@ -528,7 +652,9 @@ int resident_blocks(int prec, int variant) {
     else if (variant == 2) k = reinterpret_cast<const void*>(&direct_f32_kernel<2, true, false, false>);
     else if (variant == 3) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<1, true, false, false>);
     else if (variant == 4) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<2, true, false, false>);
-    else k = reinterpret_cast<const void*>(&direct_f32x2_kernel<3, true, false, false>);
+    else if (variant == 5) k = reinterpret_cast<const void*>(&direct_f32x2_kernel<3, true, false, false>);
+    else if (variant == 6) k = reinterpret_cast<const void*>(&direct_f32jp_kernel<1, true, false, false>);
+    else k = reinterpret_cast<const void*>(&direct_f32jp_kernel<2, true, false, false>);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kBS, 0) != cudaSuccess || nb < 1) {
         (void)cudaGetLastError();
@@ -585,7 +711,7 @@ void launch_direct(const DirectLaunch& L) {
     RRG_REQUIRE(real_splits <= 1 || (reinterpret_cast<uintptr_t>(L.scratch) & 15u) == 0,
                 RRG_ERR_INVALID, "direct sum: split partials must start on a 16-byte boundary");
     const bool usoft = (L.hsoft == nullptr);
-    const int variant = (L.prec == RRG_PREC_FP32 && L.variant >= 1 && L.variant <= 5)
+    const int variant = (L.prec == RRG_PREC_FP32 && L.variant >= 1 && L.variant <= 7)
                             ? L.variant
                             : variant_for(L.prec, L.n);
     const int ipt = L.prec == RRG_PREC_FP64 ? 1 : ipt_of(variant);
@@ -646,17 +772,34 @@ void launch_direct(const DirectLaunch& L) {
             else direct_f32x2_kernel<G, false, false, M><<<grid, kBS, 0, L.stream>>>(p);         \
         }                                                                                        \
     } while (0)
+#define RRG_JPM(G, M)                                                                            \
+    do {                                                                                         \
+        if (usoft) {                                                                             \
+            if (L.want_pot) direct_f32jp_kernel<G, true, true, M><<<grid, kBS, 0, L.stream>>>(p); \
+            else direct_f32jp_kernel<G, true, false, M><<<grid, kBS, 0, L.stream>>>(p);          \
+        } else {                                                                                 \
+            if (L.want_pot) direct_f32jp_kernel<G, false, true, M><<<grid, kBS, 0, L.stream>>>(p);\
+            else direct_f32jp_kernel<G, false, false, M><<<grid, kBS, 0, L.stream>>>(p);         \
+        }                                                                                        \
+    } while (0)
         if (variant == 3) {
             if (umass) RRG_X2M(1, true);
             else RRG_X2M(1, false);
         } else if (variant == 4) {
             if (umass) RRG_X2M(2, true);
             else RRG_X2M(2, false);
-        } else {
+        } else if (variant == 5) {
             if (umass) RRG_X2M(3, true);
             else RRG_X2M(3, false);
+        } else if (variant == 6) {
+            if (umass) RRG_JPM(1, true);
+            else RRG_JPM(1, false);
+        } else {
+            if (umass) RRG_JPM(2, true);
+            else RRG_JPM(2, false);
         }
 #undef RRG_X2M
+#undef RRG_JPM
     } else if (ipt == 1) {
         dispatch_f32<1>(usoft, mixed, L.want_pot, grid, p, L.stream);
     } else {

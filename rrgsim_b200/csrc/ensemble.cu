@@ -44,15 +44,21 @@ struct EnsForceParams {
     V4<float>* part;
 };
 
-// Persistent force kernel: G float2 groups per thread (2 G i-particles), paired FP32 ops as
-// in direct_f32x2_kernel.
+// Persistent force kernel: 2 G i-particles per thread, paired FP32 ops as in
+// direct_f32jp_kernel: each f32x2 instruction takes one i against two consecutive j, so one
+// pair of shared-memory loads feeds 2 G x 2 pairs. Shared layout per j-pair q:
+// (x_2q, x_2q+1, y_2q, y_2q+1), (z_2q, z_2q+1, m_2q, m_2q+1); the two lanes add at the end.
 // UMASS: all particles of each galaxy share its mass gg.m (multiplied in once per sum).
 template <int G, bool UMASS>
 __global__ void __launch_bounds__(kBS, 2) ens_forces_kernel(const EnsForceParams p) {
-    __shared__ float4 s_xy[kBS];
-    __shared__ float4 s_zm[kBS];
+    constexpr int IPT = 2 * G;
+    __shared__ float4 s_xy[kBS / 2];
+    __shared__ float4 s_zm[kBS / 2];
     __shared__ int s_item;
     const int tid = threadIdx.x;
+    float* const fxy = reinterpret_cast<float*>(s_xy);
+    float* const fzm = reinterpret_cast<float*>(s_zm);
+    const int q0 = tid >> 1, e0 = tid & 1;
     for (;;) {
         __syncthreads();  // previous item fully done with s_item and the tiles
         if (tid == 0) s_item = static_cast<int>(atomicAdd(p.counter, 1u));
@@ -62,78 +68,70 @@ __global__ void __launch_bounds__(kBS, 2) ens_forces_kernel(const EnsForceParams
         const EnsItem w = p.items[it];
         const EnsGalaxy gg = p.gal[w.g];
         const float2 hs = make_float2(gg.h2, gg.h2);
-        float2 nx[G], ny[G], nz[G];
+        float2 nx[IPT], ny[IPT], nz[IPT];
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-            float v[2][3];
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int li = w.i0 + (2 * g + e) * kBS + tid;
-                V4<float> pi = v4<float>(0.f, 0.f, 0.f, 0.f);
-                if (li < gg.n) pi = p.posm[gg.off + li];
-                v[e][0] = pi.x;
-                v[e][1] = pi.y;
-                v[e][2] = pi.z;
-            }
-            nx[g] = make_float2(-v[0][0], -v[1][0]);
-            ny[g] = make_float2(-v[0][1], -v[1][1]);
-            nz[g] = make_float2(-v[0][2], -v[1][2]);
+        for (int q = 0; q < IPT; ++q) {
+            const int li = w.i0 + q * kBS + tid;
+            V4<float> pi = v4<float>(0.f, 0.f, 0.f, 0.f);
+            if (li < gg.n) pi = p.posm[gg.off + li];
+            nx[q] = make_float2(-pi.x, -pi.x);
+            ny[q] = make_float2(-pi.y, -pi.y);
+            nz[q] = make_float2(-pi.z, -pi.z);
         }
-        float2 ax[G], ay[G], az[G];
+        float2 ax[IPT], ay[IPT], az[IPT];
 #pragma unroll
-        for (int g = 0; g < G; ++g) ax[g] = ay[g] = az[g] = make_float2(0.f, 0.f);
+        for (int q = 0; q < IPT; ++q) ax[q] = ay[q] = az[q] = make_float2(0.f, 0.f);
         const int je = min(w.j1, gg.n);
         V4<float> nxt = v4<float>(kPad, kPad, kPad, 0.f);
         if (w.j0 + tid < je) nxt = p.posm[gg.off + w.j0 + tid];
         for (int j0 = w.j0; j0 < je; j0 += kBS) {
             __syncthreads();
-            s_xy[tid] = make_float4(nxt.x, nxt.x, nxt.y, nxt.y);
-            s_zm[tid] = make_float4(nxt.z, nxt.z, nxt.w, nxt.w);
+            fxy[4 * q0 + e0] = nxt.x;
+            fxy[4 * q0 + 2 + e0] = nxt.y;
+            fzm[4 * q0 + e0] = nxt.z;
+            fzm[4 * q0 + 2 + e0] = nxt.w;
             __syncthreads();
             nxt = v4<float>(kPad, kPad, kPad, 0.f);
             if (j0 + kBS + tid < je) nxt = p.posm[gg.off + j0 + kBS + tid];
-            float2 tx[G], ty[G], tz[G];
+            float2 tx[IPT], ty[IPT], tz[IPT];
 #pragma unroll
-            for (int g = 0; g < G; ++g) tx[g] = ty[g] = tz[g] = make_float2(0.f, 0.f);
+            for (int q = 0; q < IPT; ++q) tx[q] = ty[q] = tz[q] = make_float2(0.f, 0.f);
 #pragma unroll 8
-            for (int k = 0; k < kBS; ++k) {
+            for (int k = 0; k < kBS / 2; ++k) {
                 const float4 xy = s_xy[k];
                 const float4 zm = s_zm[k];
                 const float2 px = make_float2(xy.x, xy.y), py = make_float2(xy.z, xy.w);
                 const float2 pz = make_float2(zm.x, zm.y), pm = make_float2(zm.z, zm.w);
 #pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    const float2 dx = __fadd2_rn(px, nx[g]);
-                    const float2 dy = __fadd2_rn(py, ny[g]);
-                    const float2 dz = __fadd2_rn(pz, nz[g]);
+                for (int q = 0; q < IPT; ++q) {
+                    const float2 dx = __fadd2_rn(px, nx[q]);
+                    const float2 dy = __fadd2_rn(py, ny[q]);
+                    const float2 dz = __fadd2_rn(pz, nz[q]);
                     const float2 r2 =
                         __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, hs)));
                     const float2 inv = make_float2(rsqrt_sfu(r2.x), rsqrt_sfu(r2.y));
                     const float2 minv = UMASS ? inv : __fmul2_rn(pm, inv);
                     const float2 kk = __fmul2_rn(minv, __fmul2_rn(inv, inv));
-                    tx[g] = __ffma2_rn(dx, kk, tx[g]);
-                    ty[g] = __ffma2_rn(dy, kk, ty[g]);
-                    tz[g] = __ffma2_rn(dz, kk, tz[g]);
+                    tx[q] = __ffma2_rn(dx, kk, tx[q]);
+                    ty[q] = __ffma2_rn(dy, kk, ty[q]);
+                    tz[q] = __ffma2_rn(dz, kk, tz[q]);
                 }
             }
 #pragma unroll
-            for (int g = 0; g < G; ++g) {
-                ax[g] = __fadd2_rn(ax[g], tx[g]);
-                ay[g] = __fadd2_rn(ay[g], ty[g]);
-                az[g] = __fadd2_rn(az[g], tz[g]);
+            for (int q = 0; q < IPT; ++q) {
+                ax[q] = __fadd2_rn(ax[q], tx[q]);
+                ay[q] = __fadd2_rn(ay[q], ty[q]);
+                az[q] = __fadd2_rn(az[q], tz[q]);
             }
         }
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int li = w.i0 + (2 * g + e) * kBS + tid;
-                if (li >= gg.n) continue;
-                const float sc = UMASS ? gg.m : 1.f;
-                p.part[gg.part_off + static_cast<int64_t>(w.s) * gg.n + li] =
-                    v4<float>(sc * (e ? ax[g].y : ax[g].x), sc * (e ? ay[g].y : ay[g].x),
-                              sc * (e ? az[g].y : az[g].x), 0.f);
-            }
+        for (int q = 0; q < IPT; ++q) {
+            const int li = w.i0 + q * kBS + tid;
+            if (li >= gg.n) continue;
+            const float sc = UMASS ? gg.m : 1.f;
+            p.part[gg.part_off + static_cast<int64_t>(w.s) * gg.n + li] =
+                v4<float>(sc * (ax[q].x + ax[q].y), sc * (ay[q].x + ay[q].y),
+                          sc * (az[q].x + az[q].y), 0.f);
         }
     }
 }

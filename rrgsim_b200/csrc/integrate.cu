@@ -2,6 +2,7 @@
 #include <cstdlib>
 
 #include "kernels.cuh"
+#include "sums.cuh"
 
 namespace rrg {
 namespace {
@@ -54,61 +55,9 @@ __global__ void correct_kernel(int64_t n, V4<R>* __restrict__ vel, const V4<R>* 
 // calc_conservation: nbody.cu:246-291; compute_center_of_mass_kernel: nbody.cu:293-396.
 // ---------------------------------------------------------------------------------------------
 constexpr int kRedThreads = 256;
-constexpr int kRedVals = 12;
 
-// The sums are double-double (Knuth TwoSum / Fast2Sum carried through every addition, rounded
-// once at the end): each result is the correctly rounded sum of the per-particle terms unless
-// that exact sum lies within about 2^-100 of its magnitude of a rounding boundary, so it does
-// not depend on the order of the particles in memory, which the cell sort changes.
-struct DD {
-    double hi, lo;
-};
-
-__device__ __forceinline__ DD dd_norm(double s, double e) {
-    const double hi = __dadd_rn(s, e);
-    return DD{hi, __dsub_rn(e, __dsub_rn(hi, s))};
-}
-
-__device__ __forceinline__ DD dd_add(DD a, double b) {
-    const double s = __dadd_rn(a.hi, b);
-    const double bb = __dsub_rn(s, a.hi);
-    const double e = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bb)), __dsub_rn(b, bb));
-    return dd_norm(s, __dadd_rn(e, a.lo));
-}
-
-__device__ __forceinline__ DD dd_add(DD a, DD b) {
-    const double s = __dadd_rn(a.hi, b.hi);
-    const double bb = __dsub_rn(s, a.hi);
-    const double e = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bb)), __dsub_rn(b.hi, bb));
-    return dd_norm(s, __dadd_rn(e, __dadd_rn(a.lo, b.lo)));
-}
-
-__device__ __forceinline__ DD warp_sum_dd(DD v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        DD w;
-        w.hi = __shfl_down_sync(0xffffffffu, v.hi, o);
-        w.lo = __shfl_down_sync(0xffffffffu, v.lo, o);
-        v = dd_add(v, w);
-    }
-    return v;
-}
-
-// Per thread each sum is cascaded (Ogita, Rump and Oishi's Sum2): s += x by TwoSum, and the
-// rounding errors add up in c, 7 FP64 operations per term; (s, c) becomes a double-double for the
-// warp, block and final reductions. partial: [nblocks][kRedVals][2] (hi, lo). COM adds the four
-// mass-centre sums (M, Mx); without it they stay 0.
-struct Casc {
-    double s, c;
-};
-
-__device__ __forceinline__ void casc_add(Casc& a, double x) {
-    const double t = __dadd_rn(a.s, x);
-    const double z = __dsub_rn(t, a.s);
-    a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, z)), __dsub_rn(x, z)));
-    a.s = t;
-}
-
+// partial: [nblocks][kRedVals][2] (hi, lo). COM adds the four mass-centre sums (M, Mx); without
+// it they stay 0.
 template <typename R, bool MIXED, bool COM>
 __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
     int64_t n, const V4<R>* __restrict__ posm, const V4<float>* __restrict__ lo,
@@ -149,19 +98,15 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
         }
         const double m = p.w;
         const double vx = v.x, vy = v.y, vz = v.z;
-        casc_add(acc[0], m * (vx * vx + vy * vy + vz * vz));
-        casc_add(acc[1], pot ? m * static_cast<double>(ph) : 0.0);
-        casc_add(acc[2], m * vx);
-        casc_add(acc[3], m * vy);
-        casc_add(acc[4], m * vz);
-        casc_add(acc[5], m * (vz * y - vy * z));
-        casc_add(acc[6], m * (vx * z - vz * x));
-        casc_add(acc[7], m * (vy * x - vx * y));
+        const double phd = pot ? static_cast<double>(ph) : 0.0;
+#pragma unroll
+        for (int k = 0; k < kConsTerms; ++k)
+            casc_add(acc[k], cons_term(k, x, y, z, m, vx, vy, vz, phd));
         if constexpr (COM) {
             casc_add(acc[8], m);
-            casc_add(acc[9], m * x);
-            casc_add(acc[10], m * y);
-            casc_add(acc[11], m * z);
+            casc_add(acc[9], __dmul_rn(m, x));
+            casc_add(acc[10], __dmul_rn(m, y));
+            casc_add(acc[11], __dmul_rn(m, z));
         }
     }
     // block partials: every thread's sums go to shared memory, then warp w reduces values
@@ -189,15 +134,29 @@ __global__ void __launch_bounds__(kRedThreads) conservation_kernel(
 
 // One block per reduced value: thread t sums block partials t, t + 256, ... in order, then a
 // fixed shuffle tree per warp and the warps in order, all in double-double; the result is its
-// rounded high part. (Summing in the last block of the main kernel instead, with the other
-// blocks counted by an atomic, measured slower: one block then does twelve blocks' work.)
+// rounded high part. Value k of block b is the double-double at
+// partial[(k kstride + b bstride) 2]; values from `nvals` on are zero. (Summing in the last
+// block of the main kernel instead, with the other blocks counted by an atomic, measured
+// slower: one block then does twelve blocks' work.)
 __global__ void __launch_bounds__(kRedThreads) conservation_finish(
-    const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+    const double* __restrict__ partial, int nblocks, int nvals, int64_t kstride,
+    int64_t bstride, double* __restrict__ out) {
     const int k = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     DD t{0.0, 0.0};
-    for (int b = threadIdx.x; b < nblocks; b += kRedThreads) {
-        const int64_t o = (static_cast<int64_t>(b) * kRedVals + k) * 2;
-        t = dd_add(t, DD{partial[o], partial[o + 1]});
+    // eight records' loads are in flight before their additions (a thread that loaded one
+    // record per addition waited out a memory latency per record)
+    constexpr int U = 8;
+    for (int b0 = threadIdx.x; b0 < nblocks && k < nvals; b0 += U * kRedThreads) {
+        DD v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u * kRedThreads;
+            const int64_t o = (k * kstride + static_cast<int64_t>(b) * bstride) * 2;
+            v[u] = b < nblocks ? DD{partial[o], partial[o + 1]} : DD{0.0, 0.0};
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (b0 + u * kRedThreads < nblocks) t = dd_add(t, v[u]);
     }
     t = warp_sum_dd(t);
     __shared__ DD s[kRedThreads / 32];
@@ -385,7 +344,15 @@ void launch_conservation(int prec, int64_t n, const void* posm, const void* posl
     }
 #undef RRG_CONS
     RRG_LAUNCHED();
-    conservation_finish<<<kRedVals, kRedThreads, 0, s>>>(partial, nblocks, out);
+    conservation_finish<<<kRedVals, kRedThreads, 0, s>>>(partial, nblocks, kRedVals, 1,
+                                                          kRedVals, out);
+    RRG_LAUNCHED();
+}
+
+void launch_conservation_finish_value_major(const double* partial, int nblocks, int nvals,
+                                            double* out, cudaStream_t s) {
+    conservation_finish<<<kRedVals, kRedThreads, 0, s>>>(partial, nblocks, nvals, nblocks, 1,
+                                                          out);
     RRG_LAUNCHED();
 }
 

@@ -71,6 +71,10 @@ void launch_conservation(int prec, int64_t n, const void* posm, const void* posl
                          const void* vel, const void* pot, double* partial, int nblocks,
                          double* out, cudaStream_t s, bool com);
 int conservation_blocks(int64_t n);
+// The second stage alone, over value-major records (the fused particle pass's PM_SUMS: value k
+// of block b at partial[(k nblocks + b) 2], nvals values): out[0..11], values from nvals on 0.
+void launch_conservation_finish_value_major(const double* partial, int nblocks, int nvals,
+                                            double* out, cudaStream_t s);
 
 // Checks of an upload of particles (rrg_load_particles) on the device. Offending indices are
 // stored as 0xffffffff - i under an atomic maximum, so 0 means none and the lowest i wins.
@@ -250,8 +254,11 @@ void launch_ngp_project(int prec, int64_t n, const void* posm, const void* poslo
                         void* phi_grid, void* acc4_grid, cudaStream_t s);
 
 // Fused particle pass of the wave strategy: optional [trilinear interp + correct] then
-// optional [predict + CIC deposit].
-enum PmMode { PM_INTERP_CORRECT = 1, PM_PREDICT_DEPOSIT = 2, PM_WRITE_SYNC = 4 };
+// optional [predict + CIC deposit]. PM_SUMS (with PM_INTERP_CORRECT | PM_WRITE_SYNC) also
+// writes each block's double-double sums of the 8 conservation terms of the synced state into
+// `partial` (value-major: [8][blocks of 256 particles][2]), for
+// launch_conservation_finish_value_major.
+enum PmMode { PM_INTERP_CORRECT = 1, PM_PREDICT_DEPOSIT = 2, PM_WRITE_SYNC = 4, PM_SUMS = 8 };
 struct PmParticleArgs {
     int prec;
     int64_t n;
@@ -267,7 +274,11 @@ struct PmParticleArgs {
     double dt;
     void* pos_out = nullptr;  // predicted positions (and MIXED low parts) go here when set,
     void* lo_out = nullptr;   // else they overwrite posm / poslo in place
+    const void* pot = nullptr;  // R[n] particle potential, read by PM_SUMS
+    double* partial = nullptr;  // PM_SUMS block records
 };
+constexpr int kPmThreads = 256;
+constexpr int kPmSumValues = 8;  // values per PM_SUMS block record
 void launch_pm_particles(const PmParticleArgs& a, int mode, cudaStream_t s);
 
 // Counting sort by CIC base cell (sort.cu): keys + histogram, exclusive scan, destinations,

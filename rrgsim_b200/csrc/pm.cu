@@ -8,11 +8,13 @@
 #include <cstdlib>
 
 #include "kernels.cuh"
+#include "sums.cuh"
 
 namespace rrg {
 namespace {
 
 constexpr double kPi = 3.14159265358979;  // the reference's PI (co_info_structs.h:7)
+static_assert(kPmSumValues == kConsTerms, "PM_SUMS records hold the 8 conservation terms");
 
 __device__ __forceinline__ int wrap_mod(int i, int n) {
     i %= n;
@@ -872,9 +874,13 @@ __global__ void __launch_bounds__(256) ngp_project_kernel(int64_t n, const void*
 //                                                                             deposit)
 // ----------------------------------------------------------------------------------------------
 template <typename R, bool MIXED, int MODE>
-__global__ void __launch_bounds__(256, 6) pm_particle_kernel(PmParticleArgs a, double scale) {
+__global__ void __launch_bounds__(kPmThreads, 6) pm_particle_kernel(PmParticleArgs a, double scale) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const bool active = i < a.n;
+    // PM_SUMS: every particle's 8 conservation terms, kept in shared memory until the block's
+    // record is formed at the end of the pass (16 KB per block, reused by the reduction)
+    constexpr bool SUMS = (MODE & PM_SUMS) != 0;
+    __shared__ double terms[SUMS ? kConsTerms : 1][SUMS ? kPmThreads : 1];
     V4<R>* posm = static_cast<V4<R>*>(a.posm);
     V4<float>* lo = static_cast<V4<float>*>(a.poslo);
     V4<R>* vel = static_cast<V4<R>*>(a.vel);
@@ -902,6 +908,17 @@ __global__ void __launch_bounds__(256, 6) pm_particle_kernel(PmParticleArgs a, d
             vx = v.x; vy = v.y; vz = v.z;
             ax = ac.x; ay = ac.y; az = ac.z;
         }
+    }
+    if constexpr (SUMS) {
+        // the synced state's terms, formed as conservation_kernel forms them (x, v and phi
+        // promoted to double); stored now, so the deposit below has the registers
+        const double ph = active ? static_cast<double>(static_cast<const R*>(a.pot)[i]) : 0.0;
+#pragma unroll
+        for (int k = 0; k < kConsTerms; ++k)
+            terms[k][threadIdx.x] =
+                active ? cons_term(k, x, y, z, m, static_cast<double>(vx),
+                                   static_cast<double>(vy), static_cast<double>(vz), ph)
+                       : 0.0;
     }
     if constexpr ((MODE & PM_PREDICT_DEPOSIT) != 0) {
         if (active) {
@@ -931,6 +948,45 @@ __global__ void __launch_bounds__(256, 6) pm_particle_kernel(PmParticleArgs a, d
         }
         cic_deposit_warp(active, x, y, z, m, a.g, scale, a.mgrid);
     }
+    if constexpr (SUMS) {
+        // the block's record, in three fixed-order stages (FP64 issue, not latency, is what
+        // this costs, so every stage keeps its warps' lanes busy): warp k sums term k, each
+        // lane 8 particles' terms (cascaded); two warps combine those 32 partials per term 4 at
+        // a time; then one lane per term adds the last 8. Records are value-major,
+        // partial[(k gridDim.x + block) 2 + {0, 1}], so the finishing kernel reads them
+        // coalesced.
+        static_assert(kPmThreads / 32 == kConsTerms, "one warp per term");
+        static_assert(sizeof(DD) * kConsTerms * 40 <= sizeof(double) * kConsTerms * kPmThreads,
+                      "the stages fit in the terms' shared memory");
+        DD (*stage)[40] = reinterpret_cast<DD (*)[40]>(&terms[0][0]);
+        __syncthreads();
+        const int t = threadIdx.x;
+        {
+            const int k = t >> 5, lane = t & 31;
+            Casc c{terms[k][lane], 0.0};
+#pragma unroll
+            for (int j = lane + 32; j < kPmThreads; j += 32) casc_add(c, terms[k][j]);
+            __syncthreads();  // every term read before the stages overwrite them
+            stage[k][lane] = dd_norm(c.s, c.c);
+        }
+        __syncthreads();
+        if (t < 64) {
+            const int k = t >> 3, q = t & 7;
+            DD d = stage[k][4 * q];
+#pragma unroll
+            for (int j = 1; j < 4; ++j) d = dd_add(d, stage[k][4 * q + j]);
+            stage[k][32 + q] = d;
+        }
+        __syncthreads();
+        if (t < kConsTerms) {
+            DD d = stage[t][32];
+#pragma unroll
+            for (int j = 1; j < 8; ++j) d = dd_add(d, stage[t][32 + j]);
+            const int64_t o = (static_cast<int64_t>(t) * gridDim.x + blockIdx.x) * 2;
+            a.partial[o] = d.hi;
+            a.partial[o + 1] = d.lo;
+        }
+    }
 }
 
 template <typename R, bool MIXED>
@@ -948,6 +1004,11 @@ void dispatch_pm(const PmParticleArgs& a, int mode, double scale, cudaStream_t s
             break;
         case PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT | PM_WRITE_SYNC:
             pm_particle_kernel<R, MIXED, PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT | PM_WRITE_SYNC>
+                <<<b, 256, 0, s>>>(a, scale);
+            break;
+        case PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT | PM_WRITE_SYNC | PM_SUMS:
+            pm_particle_kernel<R, MIXED,
+                               PM_INTERP_CORRECT | PM_PREDICT_DEPOSIT | PM_WRITE_SYNC | PM_SUMS>
                 <<<b, 256, 0, s>>>(a, scale);
             break;
         default:

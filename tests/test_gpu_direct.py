@@ -215,6 +215,53 @@ def test_asynchronous_conservation_sums_equal_the_synchronous_ones(memory):
         np.testing.assert_array_equal(got["angular"], ref["angular"])
 
 
+_VARIANT_SCRIPT = r"""
+import json, sys
+import numpy as np
+sys.path[:0] = sys.argv[1:3]
+import oracle as orc
+import rrgsim_b200 as rg
+from helpers import plummer, rel_err
+out = {}
+for n, uniform in ((1000, True), (20000, True), (5001, False)):
+    pos, vel, m, s2 = plummer(n, seed=n)
+    if not uniform:  # masses and softenings vary: the kernels without the uniform shortcuts
+        m = m * np.linspace(0.5, 1.5, n)
+        s2 = s2 * np.linspace(0.5, 2.0, n)
+    c = rg.Context(0, "fp32")
+    c.load_particles(pos, vel, m, s2)
+    c.nbody_acceleration()
+    acc = c.get_particles()["acc"]
+    c.nbody_grav()
+    grav = c.get_particles()["grav"]
+    c.close()
+    g = orc.direct_grav(pos, m, s2)
+    out[f"{n}"] = [float(np.median(rel_err(acc, orc.direct_acc(pos, m, s2)))),
+                   float(np.median(np.abs(grav - g) / np.abs(g)))]
+print(json.dumps(out))
+"""
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
+def test_every_fp32_kernel_variant_matches_oracle(variant):
+    """Each FP32 direct-sum kernel (scalar with 1 or 2 i-particles per thread; paired over i
+    with 2, 4 or 6; paired over j with 1 or 2), chosen by RRG_DIRECT_VARIANT, which is read once
+    per process: accelerations and potentials at sizes with one and several j-splits, with
+    uniform and with varying masses and softenings, against the FP64 oracle."""
+    import json
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    env = dict(os.environ, RRG_DIRECT_VARIANT=str(variant))
+    r = subprocess.run([sys.executable, "-c", _VARIANT_SCRIPT, here, os.path.dirname(here)],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    errs = json.loads(r.stdout.strip().splitlines()[-1])
+    for n, (ea, eg) in errs.items():
+        assert ea <= 1e-5 and eg <= 1e-5, (variant, n, ea, eg)
+
+
 @pytest.mark.parametrize("n", [3000, 3001, 65537])
 def test_raw_device_entry_points_match_context(n):
     # n = 3001 and 65537 (n % 4 != 0, several j-splits): the split partials must still start

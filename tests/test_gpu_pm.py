@@ -384,6 +384,60 @@ def test_step_by_step_calls_equal_one_long_call(prec, interval):
         np.testing.assert_array_equal(gr["grav"], out[0][1]["grav"])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "mixed", "fp64"])
+def test_step_sums_equal_a_pass_over_the_particles(prec):
+    """With set_step_sums the last particle pass of each calc_steps call also forms the
+    conservation sums (nbody.cu:246-291) of the state it leaves, and a calc_conservation or
+    calc_conservation_async right after the call only combines them: one kernel instead of two.
+    The sums equal those of the pass over the particles bit for bit, the steps do not change,
+    and a call that may change the state in between (here the sync, which rewrites the
+    particles' potential) makes the sums come from the particles again."""
+    torch = pytest.importorskip("torch")
+    nx, n, dt = 32, 20000, 2e-3
+    pos, vel, m, s2 = disk(n, seed=5)
+    m = m * np.linspace(0.5, 1.5, n)
+    g = _grid(nx)
+    vmax = np.max(np.linalg.norm(vel, axis=1))
+    wp = rg.WaveParams.make(g.dx, diss_base=1.0 / (4 * g.dx), wave_speed=10 * vmax,
+                            iterations=20, setup_iterations=200, steady_check_step=1000)
+    sim = rg.SimParams(time_max=1.0, dt_save=0.1, dt_dynamics=dt, saves_without_dump=2 ** 63,
+                       use_wave_model=1)
+    calls = [1, 1, 3, 1, 6, 1]  # sorts (every 4 steps) fall inside and between calls
+    res = {}
+    for on in (False, True):
+        sums = torch.full((len(calls), 12), float("nan"), dtype=torch.float64).pin_memory().numpy()
+        rows, launches = [], []
+        with _ctx(prec, pos, vel, m, s2, g) as c:
+            c.set_sort_interval(4)
+            c.set_wave_params(wp)
+            c.solver_init(sim)
+            c.precalc()
+            c.sync_particles_and_grid()  # a potential on the particles: Ep is not zero
+            c.set_step_sums(on)
+            for k, steps in enumerate(calls):
+                c.calc_steps(steps)
+                if k == 3:
+                    c.sync_particles_and_grid()
+                l0 = rg.kernel_launch_count()
+                c.calc_conservation_async(sums[k])
+                rows.append(c.calc_conservation())
+                launches.append(rg.kernel_launch_count() - l0)
+            c.synchronize()
+            res[on] = (rows, launches, sums.copy(), c.get_particles())
+    rows_off, launches_off, sums_off, p_off = res[False]
+    rows_on, launches_on, sums_on, p_on = res[True]
+    assert launches_off == [4] * len(calls)
+    assert launches_on == [2, 2, 2, 4, 2, 2]
+    assert rows_on[0]["Ep"] != 0.0
+    for a, b in zip(rows_off, rows_on):
+        assert a["Ek"] == b["Ek"] and a["Ep"] == b["Ep"]
+        np.testing.assert_array_equal(a["momentum"], b["momentum"])
+        np.testing.assert_array_equal(a["angular"], b["angular"])
+    np.testing.assert_array_equal(sums_off, sums_on)
+    for k in ("pos", "vel", "acc"):
+        np.testing.assert_array_equal(p_off[k], p_on[k])
+
+
 @pytest.mark.parametrize("prec", ["fp32", "mixed"])
 @pytest.mark.parametrize("nx,iterations", [(32, 20), (64, 7), (64, 1), (128, 20), (128, 7),
                                            (128, 1)])

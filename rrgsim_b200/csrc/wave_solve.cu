@@ -42,7 +42,18 @@
 //   loads its share, re-reads any float4 still empty and empties the slot, and a fence per
 //   thread orders those resets before its next face stores. The same bits, but 103-108 against
 //   98 us per launch (the resets double the stores to L2; with face stores after the planes or
-//   interleaved, with or without a back-off in the poll, all within 1%).
+//   interleaved, with or without a back-off in the poll, all within 1%);
+// - clusters of 4 x 2 blocks (y x z; 32 of them resident with the cooperative launch): faces
+//   between partners pushed straight into the partner's tile and z halo between two cluster
+//   barriers per substep, only the cluster's boundary faces through L2 (4 or 8 KB per block
+//   instead of 16, one or two counters instead of four). The same bits, but 112.8 against 96.9
+//   us per launch: the two cluster barriers add more than the smaller exchange saves.
+//
+// Timing-only copies (results wrong on purpose) split the launch: without the stencil
+// arithmetic it takes 79.8 us against 98.0, so the 20 exchanges, the prologue and the gradient
+// cost ~80 us and the stencil ~18 us (0.9 us per substep). The two-substep kernel without its
+// arithmetic takes 74.7 us: its 10 exchanges (two cells deep, eight neighbours) cost about as
+// much as the 20 one-deep ones.
 //
 // All blocks must be resident together: the launch is cooperative and the host checks capacity
 // first. Every wait is bounded; one that runs out sets the error word and the block leaves (the

@@ -43,7 +43,8 @@ __device__ __forceinline__ void interp_axis_w(double x, double dmin, double dx, 
     i1 = max(0, min(a + 1, nx - 1));
 }
 
-// interp adjoint: gbar += T(x)^T A (atomics, when gbar != nullptr); X = sum dW/dx (g . A)
+// interp adjoint: gbar += T(x)^T A (atomics, when gbar != nullptr; gbar holds 4 values per
+// cell, the fourth unused); X = sum dW/dx (g . A)
 template <typename R>
 __global__ void __launch_bounds__(256) interp_adjoint_kernel(int64_t n, const V4<R>* __restrict__ posm,
                                                              GridDev g, const V4<R>* __restrict__ acc4,
@@ -79,9 +80,15 @@ __global__ void __launch_bounds__(256) interp_adjoint_kernel(int64_t n, const V4
                 gz += wxs[i] * wys[j] * dws[k] * s;
                 if (gbar) {
                     const R W = wxs[i] * wys[j] * wzs[k];
-                    atomicAdd(gbar + 3 * c, W * a.x);
-                    atomicAdd(gbar + 3 * c + 1, W * a.y);
-                    atomicAdd(gbar + 3 * c + 2, W * a.z);
+                    if constexpr (sizeof(R) == 4) {
+                        // one 16-byte vector atomic per corner instead of three scalar ones
+                        atomicAdd(reinterpret_cast<float4*>(gbar) + c,
+                                  make_float4(W * a.x, W * a.y, W * a.z, 0.f));
+                    } else {
+                        atomicAdd(gbar + 4 * c, W * a.x);
+                        atomicAdd(gbar + 4 * c + 1, W * a.y);
+                        atomicAdd(gbar + 4 * c + 2, W * a.z);
+                    }
                 }
             }
     X[p] = v4<R>(gx, gy, gz, R(0));
@@ -91,10 +98,10 @@ __global__ void __launch_bounds__(256) interp_adjoint_kernel(int64_t n, const V4
 template <typename R>
 __device__ __forceinline__ R dT_axis(const R* gb, int comp, int64_t c, int j, int n, int64_t st) {
     R s = 0;
-    if (j - 1 >= 0) s += (j - 1 == 0 ? R(1) : R(0.5)) * gb[3 * (c - st) + comp];
-    if (j + 1 <= n - 1) s -= (j + 1 == n - 1 ? R(1) : R(0.5)) * gb[3 * (c + st) + comp];
-    if (j == 0) s -= gb[3 * c + comp];
-    if (j == n - 1) s += gb[3 * c + comp];
+    if (j - 1 >= 0) s += (j - 1 == 0 ? R(1) : R(0.5)) * gb[4 * (c - st) + comp];
+    if (j + 1 <= n - 1) s -= (j + 1 == n - 1 ? R(1) : R(0.5)) * gb[4 * (c + st) + comp];
+    if (j == 0) s -= gb[4 * c + comp];
+    if (j == n - 1) s += gb[4 * c + comp];
     return s;
 }
 
@@ -437,7 +444,7 @@ RRG_API rrg_status rrg_pm_adjoint_create(int device, int precision, int64_t n, d
         P->mg.alloc(8 * P->nc);
         for (PBuf* b : {&P->src, &P->phi[0], &P->phi[1], &P->Cb, &P->Pb, &P->F}) b->alloc(gb);
         P->acc4.alloc(4 * gb);
-        P->gbar.alloc(3 * gb);
+        P->gbar.alloc(4 * gb);
         const int nck = (nsteps + P->every - 1) / P->every;
         P->ck_x.alloc(pb * nck);
         P->ck_v.alloc(pb * nck);

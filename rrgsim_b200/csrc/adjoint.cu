@@ -82,10 +82,13 @@ __device__ __forceinline__ void adjoint_update_at(int64_t i, R xx, R xy, R xz,
     u.c[i] = v4<R>(cx, cy, cz, R(0));
 }
 
+// FP64: CUDA's rsqrt (within 1 ulp) instead of the forward's 1 / sqrt, whose square root and
+// division each cost a Newton sequence; the VJP's pair loop is FP64-pipe bound, and the
+// difference (a few 1e-16 relative per pair) is far below what any FP64 check resolves
 template <typename R>
 __device__ __forceinline__ R inv_sqrt(R x) {
     if constexpr (sizeof(R) == 4) return rsqrt_sfu(x);
-    else return R(1) / sqrt(x);
+    else return rsqrt(x);
 }
 
 // ----------------------------------------------------------------------------------------------

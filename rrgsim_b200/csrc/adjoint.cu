@@ -339,8 +339,8 @@ __global__ void __launch_bounds__(kBS) vjp_sym_kernel(const VjpSymParams<R> p) {
     __syncthreads();
     const bool sym = (a != b);
     R gx = 0, gy = 0, gz = 0, gm = 0;
-#pragma unroll 2
-    for (int q = 0; q < kBS; ++q) {
+    // one pair (k, j): its k-side terms into (gx, gy, gz, gm), its j-side ones returned
+    auto pair = [&](int q, R& jx, R& jy, R& jz, R& jm) {
         const V4<R> pj = s_pos[q];
         const V4<R> lj = s_lam[q];
         const R dx = pj.x - pk.x, dy = pj.y - pk.y, dz = pj.z - pk.z;
@@ -359,16 +359,38 @@ __global__ void __launch_bounds__(kBS) vjp_sym_kernel(const VjpSymParams<R> p) {
         gy += Ty;
         gz += Tz;
         gm -= f * (dx * lj.x + dy * lj.y + dz * lj.z);
-        if (sym) {
-            // j-side: -T and + f (lam_k . d), summed over the warp, one shared add per warp
-            const R jx = warp_sum_r(-Tx), jy = warp_sum_r(-Ty), jz = warp_sum_r(-Tz);
-            const R jm = warp_sum_r(f * (dx * lk.x + dy * lk.y + dz * lk.z));
-            if (lane == 0) {
-                atomicAdd(&s_acc[q][0], jx);
-                atomicAdd(&s_acc[q][1], jy);
-                atomicAdd(&s_acc[q][2], jz);
-                atomicAdd(&s_acc[q][3], jm);
+        jx = -Tx;
+        jy = -Ty;
+        jz = -Tz;
+        jm = f * (dx * lk.x + dy * lk.y + dz * lk.z);
+    };
+    if (!sym) {
+#pragma unroll 2
+        for (int q = 0; q < kBS; ++q) {
+            R jx, jy, jz, jm;
+            pair(q, jx, jy, jz, jm);
+        }
+    } else {
+        // the j-side terms ride along the warp: in step t of a chunk of 32 j, lane l takes
+        // j = 32 c + (l + t) mod 32 and adds to the sums that lane l + 1 held for it, so after
+        // 32 steps lane l holds its warp's sums for j = 32 c + l (one shuffle per sum and step,
+        // and one shared add per chunk, instead of a warp reduction per j)
+        for (int c = 0; c < kBS / 32; ++c) {
+            R ax = 0, ay = 0, az = 0, am = 0;
+#pragma unroll 4
+            for (int t = 0; t < 32; ++t) {
+                R jx, jy, jz, jm;
+                pair(c * 32 + ((lane + t) & 31), jx, jy, jz, jm);
+                const int from = (lane + 1) & 31;
+                ax = __shfl_sync(0xffffffffu, ax + jx, from);
+                ay = __shfl_sync(0xffffffffu, ay + jy, from);
+                az = __shfl_sync(0xffffffffu, az + jz, from);
+                am = __shfl_sync(0xffffffffu, am + jm, from);
             }
+            atomicAdd(&s_acc[c * 32 + lane][0], ax);
+            atomicAdd(&s_acc[c * 32 + lane][1], ay);
+            atomicAdd(&s_acc[c * 32 + lane][2], az);
+            atomicAdd(&s_acc[c * 32 + lane][3], am);
         }
     }
     p.slots[(a * T + b) * kBS + tid] = v4<R>(gx, gy, gz, gm);

@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kThreads, 2) wave_solve_kernel(const SolveArgs
     const float4* const c4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi0 : a.phi1);
     const float4* const p4 = reinterpret_cast<const float4*>(a.cur == 0 ? a.phi1 : a.phi0);
     const ulonglong2* const m2 = reinterpret_cast<const ulonglong2*>(a.mg);
-    float4 cur[ZC], old[ZC];
+    float4 cur[ZC], old[ZC] = {};  // (old: set before the first substep)
 #pragma unroll
     for (int k = 0; k < ZC; ++k) {
         cur[k] = __ldcg(c4 + col + k * plane4);

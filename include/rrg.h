@@ -160,7 +160,13 @@ RRG_API uint64_t rrg_kernel_launch_count(void);
 RRG_API rrg_status rrg_create(int device, int precision, rrg_ctx** out);
 RRG_API rrg_status rrg_destroy(rrg_ctx* ctx);
 
-/* Makes the context launch on `stream` (a cudaStream_t; NULL = the context's own stream). */
+/* Makes the context launch on `stream` (a cudaStream_t; NULL = the context's own stream).
+ * Once the context has a grid, the stream it launches on carries a persisting L2
+ * access-policy window over the context's deposit grids and wave levels (48 MB at 128^3), and
+ * the process's persisting L2 set-aside is sized to it: every PM step reads and rewrites those
+ * grids, and keeping them in L2 shortens the step by ~3%. The window moves with the context to
+ * a new stream, and rrg_destroy takes it off a caller's stream. Environment RRG_L2_PERSIST=0
+ * leaves L2 alone. */
 RRG_API rrg_status rrg_set_stream(rrg_ctx* ctx, void* stream);
 RRG_API rrg_status rrg_synchronize(rrg_ctx* ctx);
 

@@ -333,9 +333,10 @@ def run_native(args):
     # (per substep read phi^n, phi^n-1, the source and write phi^n+1: 16 B/cell; the deposit's
     # clear and write: 8 + 8; the gradient's read of phi, 12). The solve launch does the
     # substeps, the clear and the gradient: 340 B/cell. Its substeps stay on chip and in L2, so
-    # this rate may exceed the HBM copy peak; the bytes that must reach DRAM once per launch
-    # (deposit in 8, other deposit cleared 8, source out 4, both levels in and out 16, field out
-    # 16: 52 B/cell) and ncu's DRAM bytes are reported beside it.
+    # this rate may exceed the HBM copy peak; the bytes that would reach DRAM once per launch
+    # with nothing kept in L2 between launches (deposit in 8, other deposit cleared 8, source
+    # out 4, both levels in and out 16, field out 16: 52 B/cell; the persisting L2 window keeps
+    # the deposits and levels, 40 of them, on chip) and ncu's DRAM bytes are reported beside it.
     alg_bytes = (20 * 16 + 8 + 12) * cells
     min_bytes = 52 * cells
     step_bytes = 52 * N_PART + (20 * 16 + 16 + 12) * cells

@@ -47,7 +47,9 @@
 //   between partners pushed straight into the partner's tile and z halo between two cluster
 //   barriers per substep, only the cluster's boundary faces through L2 (4 or 8 KB per block
 //   instead of 16, one or two counters instead of four). The same bits, but 112.8 against 96.9
-//   us per launch: the two cluster barriers add more than the smaller exchange saves.
+//   us per launch: the two cluster barriers add more than the smaller exchange saves;
+// - relaxed loads in the poll and one acquire fence after it instead of acquire loads: 100.2
+//   against 92.7 us per launch (the fence costs more than the acquire loads).
 //
 // Timing-only copies (results wrong on purpose) split the launch: without the stencil
 // arithmetic it takes 79.8 us against 98.0, so the 20 exchanges, the prologue and the gradient

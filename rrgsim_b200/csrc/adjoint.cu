@@ -277,8 +277,9 @@ __global__ void __launch_bounds__(kBS, 2) vjp_f32x2_kernel(const VjpParams<float
 // Symmetric VJP: the pair term is antisymmetric (T_jk = -T_kj for x-bar), so each unordered
 // pair of particles is evaluated once. Blocks run over tile pairs (a, b), a <= b, of 256
 // particles: threads own k in tile a, tile b sits in shared memory. For a < b the j-side sums
-// (x-bar_j -= T, m-bar_j += f (lam_k . d)) are reduced over the warp with shuffles and added
-// into a shared accumulator; block (a, b) then writes its tile-a sums to slot [a][b] and its
+// (x-bar_j -= T, m-bar_j += f (lam_k . d)) travel along the warp with the j they belong to (one
+// shuffle per sum and step, see the kernel) and each warp adds its sums for a chunk of 32 j into
+// a shared accumulator; block (a, b) then writes its tile-a sums to slot [a][b] and its
 // tile-b sums to slot [b][a]. A finish pass adds the T slots of each particle in order
 // (deterministic). Diagonal tiles evaluate only the k-side, as a non-symmetric pass would.
 template <typename R>
@@ -292,12 +293,6 @@ struct VjpSymParams {
     V4<R>* slots;  // [tiles][tiles][256]
 };
 
-template <typename R>
-__device__ __forceinline__ R warp_sum_r(R v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 template <typename R, bool USOFT>
 __global__ void __launch_bounds__(kBS) vjp_sym_kernel(const VjpSymParams<R> p) {
